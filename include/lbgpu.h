@@ -1,0 +1,149 @@
+/* lbgpu.h -- native C interface of liblbgpu.so beyond the drop-in lb.h / boundaries.h.
+ *
+ * Two groups of functions:
+ *
+ *  1. Companions of the drop-in interface (no counterpart in the reference, whose lattice
+ *     lives in host memory only): copying the device lattice back, telling the library the
+ *     host copy changed, choosing what is copied back after each entry point, and reading
+ *     the error the last entry point recorded.
+ *
+ *  2. The lattice object used by benchmarks, batching and serving: populations stored in
+ *     FP64, FP32, or FP16/BF16 offsets, stepped by the two-buffer pull kernel or the in-place
+ *     AA kernel.  Geometry is given in the same per-node tag / per-side table form the
+ *     drop-in interface derives from Dynamics pointers:
+ *       tag[X*(ly+2) + Y]          X = 0..lx+1, Y = 0..ly+1 (ghost ring tag LBGPU_TAG_NONE)
+ *       bc[((t*2)+k)*nb + coord]   nb = max(lx,ly)+2; table t = family*4 + side with family
+ *                                  0 velocity (k: ux, uy) or 1 pressure (k: rho, uPar), side
+ *                                  0 upper, 1 lower, 2 left, 3 right; coord = X for upper and
+ *                                  lower, Y for left and right
+ *       populations f[((X*(ly+2)) + Y)*9 + i], the reference's node order and direction order.
+ *
+ * All functions return LB_OK (0) or an LB_ERR_* code and never abort; the message of the
+ * last failure on the calling thread is lbGetLastErrorString().
+ */
+#ifndef LBGPU_H
+#define LBGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "lb.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes ------------------------------------------------------------------- */
+enum {
+    LB_OK = 0,
+    LB_ERR_CUDA = 1,          /* a CUDA call failed (message has the CUDA error string)  */
+    LB_ERR_ALLOC = 2,         /* device or pinned-host allocation refused                 */
+    LB_ERR_ARG = 3,           /* invalid argument (size, pointer, enum value)             */
+    LB_ERR_BLOCK_SIZE = 4,    /* blk_size does not divide the swept extent                */
+    LB_ERR_DYNAMICS = 5,      /* a node uses a dynamics function the GPU cannot run       */
+    LB_ERR_LAYOUT = 6,        /* two boundary nodes share a table slot with different data */
+    LB_ERR_STATE = 7,         /* call not valid in the lattice's current state            */
+    LB_ERR_NO_DEVICE = 8,     /* no CUDA device                                           */
+    LB_ERR_TIMEOUT = 9,       /* a bounded device wait gave up                            */
+    LB_ERR_CAPACITY = 10      /* a request exceeds a fixed capacity (budget, slots)       */
+};
+
+/* Error recorded by the calling thread's most recent failing call (0 when none), and
+ * its message.  lbClearError resets both. No counterpart in the reference (void API). */
+int lbGetLastError(void);
+const char *lbGetLastErrorString(void);
+void lbClearError(void);
+
+/* ---- drop-in companions ---------------------------------------------------------- */
+/* What the drop-in entry points copy back to the host lattice after running:
+ *   LB_SYNC_NONE     nothing; call lbSyncToHost before reading sim->lattice.
+ *   LB_SYNC_OUTLET   columns lx-1 and lx-2 (interior rows), which the application driver's
+ *                    zero-gradient update reads before every step (default).
+ *   LB_SYNC_FULL     the whole current lattice, ghost ring included.
+ * The environment variable LBGPU_SYNC=none|outlet|full sets the default. */
+enum { LB_SYNC_NONE = 0, LB_SYNC_OUTLET = 1, LB_SYNC_FULL = 2 };
+void lbSetSyncMode(Simulation *sim, int mode);
+
+/* Copy the current lattice (post-stream state, ghost ring included) into the host
+ * arrays sim->lattice points to.  The host copy of tmpLattice is not maintained. */
+void lbSyncToHost(Simulation *sim);
+
+/* The driver wrote populations of sim->lattice directly: upload them before the next
+ * entry point.  (setDynamics marks the dynamics dirty by itself.) */
+void lbMarkHostDirty(Simulation *sim);
+
+/* ---- lattice object ------------------------------------------------------------------ */
+enum { LBGPU_F64 = 0, LBGPU_F32 = 1, LBGPU_F16 = 2, LBGPU_BF16 = 3 };
+enum { LBGPU_PULL = 0, LBGPU_AA = 1 };
+
+enum {
+    LBGPU_TAG_NONE = 0, LBGPU_TAG_BGK = 1, LBGPU_TAG_BOUNCE_BACK = 2,
+    LBGPU_TAG_UPPER_ZOUHE = 3, LBGPU_TAG_LOWER_ZOUHE = 4,
+    LBGPU_TAG_LEFT_ZOUHE = 5, LBGPU_TAG_RIGHT_ZOUHE = 6,
+    LBGPU_TAG_UPPER_PRESSURE_ZOUHE = 7, LBGPU_TAG_LOWER_PRESSURE_ZOUHE = 8,
+    LBGPU_TAG_LEFT_PRESSURE_ZOUHE = 9, LBGPU_TAG_RIGHT_PRESSURE_ZOUHE = 10,
+    LBGPU_TAG_UPPER_REGULARIZED = 11, LBGPU_TAG_LOWER_REGULARIZED = 12,
+    LBGPU_TAG_LEFT_REGULARIZED = 13, LBGPU_TAG_RIGHT_REGULARIZED = 14,
+    LBGPU_TAG_UPPER_PRESSURE_REGULARIZED = 15, LBGPU_TAG_LOWER_PRESSURE_REGULARIZED = 16,
+    LBGPU_TAG_LEFT_PRESSURE_REGULARIZED = 17, LBGPU_TAG_RIGHT_PRESSURE_REGULARIZED = 18,
+    LBGPU_NUM_TAGS = 19
+};
+
+enum { LBGPU_WALL_REGULARIZED = 0, LBGPU_WALL_BOUNCEBACK = 1 };
+enum { LBGPU_OUTLET_ZGB = 0, LBGPU_OUTLET_CONST = 1 };
+
+typedef struct lbgpu_lattice lbgpu_lattice;
+
+/* Allocate a lattice on the current CUDA device: two population buffers for
+ * LBGPU_PULL, one for LBGPU_AA, plus tags and tables. */
+int lbgpu_create(int lx, int ly, int precision, int scheme, lbgpu_lattice **out);
+int lbgpu_destroy(lbgpu_lattice *lat);
+
+/* Geometry and boundary data (layouts above).  zgb_row may be NULL; rows flagged there take
+ * their right-side pressure density from the zero-gradient extrapolation
+ * 4/3 rho(lx-1) - 1/3 rho(lx-2) of the populations entering each step. */
+int lbgpu_set_geometry(lbgpu_lattice *lat, double omega, const uint8_t *tag, const double *bc,
+                       const uint8_t *zgb_row);
+
+/* Initial populations of the first and second buffers (tmp may be NULL for zeros); resets
+ * the step count.  For FP16/BF16 storage, `scale_log2` in lbgpu_set_offset_scale applies. */
+int lbgpu_set_populations(lbgpu_lattice *lat, const double *f, const double *tmp);
+
+/* Power-of-two scale s of the FP16/BF16 offset storage: stored = (f_i - w_i) * 2^s. */
+int lbgpu_set_offset_scale(lbgpu_lattice *lat, int scale_log2);
+
+/* Cylinder channel on the device without host population arrays: tags and tables as the
+ * application driver builds them (obstacle disk, walls, Poiseuille inlet, pressure outlet)
+ * and equilibrium populations at rho = 1 and the Poiseuille profile.  Returns omega through
+ * omega_out when not NULL. */
+int lbgpu_setup_cylinder(lbgpu_lattice *lat, int obst_x, int obst_y, int obst_r, double umax,
+                         double re, int wall_kind, int outlet_kind, double *omega_out);
+
+/* The same geometry into host arrays (tag, bc, zgb_row, f as laid out above); f may be NULL. */
+double lbgpu_build_cylinder(int lx, int ly, int obst_x, int obst_y, int obst_r, double umax,
+                            double re, int wall_kind, int outlet_kind, uint8_t *tag,
+                            double *bc, uint8_t *zgb_row, double *f);
+
+/* Advance `nsteps` time steps; asynchronous on the lattice's stream. */
+int lbgpu_step(lbgpu_lattice *lat, int nsteps);
+
+/* Advance `nsteps` steps and report their device time in milliseconds (CUDA events on the
+ * lattice's stream); synchronous. */
+int lbgpu_step_timed(lbgpu_lattice *lat, int nsteps, float *ms);
+
+/* Current post-stream populations as FP64, ghost ring included (layout above). */
+int lbgpu_get_populations(lbgpu_lattice *lat, double *f);
+
+/* Density and velocity of the current state for the interior, [Y-1][X-1] row-major
+ * (ly rows of lx values), computed on the device. Any pointer may be NULL. */
+int lbgpu_get_macros(lbgpu_lattice *lat, double *rho, double *ux, double *uy);
+
+int lbgpu_synchronize(lbgpu_lattice *lat);
+void *lbgpu_stream(lbgpu_lattice *lat);           /* the lattice's cudaStream_t            */
+long long lbgpu_steps_done(lbgpu_lattice *lat);
+size_t lbgpu_device_bytes(lbgpu_lattice *lat);     /* device memory held by the lattice     */
+int lbgpu_last_kernel_launches(lbgpu_lattice *lat); /* kernels launched by the last step call */
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,67 @@
+// lattice.h -- the device lattice object behind both C interfaces.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+#include <vector>
+#include "kernels.h"
+
+namespace lbgpu {
+
+// Thread-local error state of the C interfaces (LB_ERR_* codes of include/lbgpu.h).
+int set_error(int code, const char *fmt, ...);
+int cuda_error(cudaError_t e, const char *what);
+int last_error();
+const char *last_error_string();
+void clear_error();
+
+enum { FORM_L = 0, FORM_C = 1 };
+
+struct Lattice {
+    int lx = 0, ly = 0;
+    int precision = 0;   // LBGPU_F64 / F32 / F16 / BF16
+    int scheme = 0;      // LBGPU_PULL / LBGPU_AA
+    DevLattice d{};
+    size_t elem = 8;     // bytes per stored population
+    int cur = 0;         // buffer holding the state
+    int form = FORM_L;   // see kernels_f64.cu
+    int pending = 0;     // form C only: 1 when the post-stream state is the current one
+    long long n = 0;     // index of the last collision (form C) or of the state (form L)
+    bool ghosts = false; // keep the ghost ring exact (drop-in interface)
+    bool zgb_each_step = false;  // native: extrapolated outlet before every step
+    cudaStream_t stream = nullptr;
+    size_t bytes = 0;
+    int launches = 0;    // kernels launched by the last public call
+
+    std::vector<double> bc_host;   // [16*nb] last uploaded boundary tables
+    std::vector<int> zgb_src_host; // [4*nb]
+    double *stage = nullptr;       // device staging for record transfers
+    size_t stage_bytes = 0;
+
+    int create(int lx, int ly, int precision, int scheme);
+    void destroy();
+
+    // per-step operations (asynchronous on `stream`)
+    int op_collide();        // collide the current state in place or through the pull kernel
+    int op_propagate();      // mark (or perform) the stream
+    int materialize();       // form C + pending -> form L
+    int zgb_pass();          // extrapolated outlet densities into the tables (zgb_src slots)
+    int step(int nsteps);    // full native steps
+
+    // data movement
+    int upload_bc(const double *bc);      // host [16*nb]
+    int upload_zgb_src(const int *src);   // host [4*nb]
+    int upload_tags(const uint8_t *tag_xy);  // host tag[X*(ly+2)+Y]
+    int upload_tag_plane(const uint8_t *plane);  // host plane in device layout
+    int upload_records(int b, const double *host, int rs, int X0, int X1);
+    int readout_records(double *host, int rs, const uint64_t *dynp_dev, int X0, int X1);
+    int init_side_from(int b, int par);
+    int init_cylinder(double umax);  // equilibrium Poiseuille populations into buffer 0
+    int get_macros(double *rho, double *ux, double *uy);  // host [ly][lx] arrays
+    int check(const char *what);   // cudaGetLastError -> error code
+    int side_par_stale() const { return (int)((n + 1) & 1); }
+    size_t stage_cols(int rs) const;
+    int ensure_stage(size_t bytes_needed);
+};
+
+}  // namespace lbgpu

@@ -1,0 +1,197 @@
+// native.cu -- the lbgpu_* functions of include/lbgpu.h (lattice object interface).
+#include <cstring>
+#include <vector>
+#include "lattice.h"
+#include "lbgpu.h"
+
+using lbgpu::Lattice;
+using lbgpu::set_error;
+
+struct lbgpu_lattice {
+    Lattice L;
+};
+
+namespace {
+
+int bad_handle(const lbgpu_lattice *h, const char *fn)
+{
+    if (!h) return set_error(LB_ERR_ARG, "%s: null lattice", fn);
+    return LB_OK;
+}
+
+// zgb_src for the native interface: right-side pressure slot Y takes row Y's extrapolation.
+void zgb_slots_from_rows(const Lattice &L, const uint8_t *zgb_row, std::vector<int> &src,
+                         bool &any)
+{
+    const int nb = L.d.g.nb;
+    src.assign(4 * (size_t)nb, -1);
+    any = false;
+    if (!zgb_row) return;
+    for (int Y = 0; Y < L.ly + 2; ++Y)
+        if (zgb_row[Y]) {
+            src[(size_t)3 * nb + Y] = Y;   // table 4 + right side -> index 3 of the 4 pressure tables
+            any = true;
+        }
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbGetLastError(void) { return lbgpu::last_error(); }
+const char *lbGetLastErrorString(void) { return lbgpu::last_error_string(); }
+void lbClearError(void) { lbgpu::clear_error(); }
+
+int lbgpu_create(int lx, int ly, int precision, int scheme, lbgpu_lattice **out)
+{
+    if (!out) return set_error(LB_ERR_ARG, "lbgpu_create: null output pointer");
+    *out = nullptr;
+    lbgpu_lattice *h = new lbgpu_lattice;
+    int rc = h->L.create(lx, ly, precision, scheme);
+    if (rc != LB_OK) {
+        h->L.destroy();
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return LB_OK;
+}
+
+int lbgpu_destroy(lbgpu_lattice *h)
+{
+    if (!h) return LB_OK;
+    h->L.destroy();
+    delete h;
+    return LB_OK;
+}
+
+int lbgpu_set_geometry(lbgpu_lattice *h, double omega, const uint8_t *tag, const double *bc,
+                       const uint8_t *zgb_row)
+{
+    if (int rc = bad_handle(h, "lbgpu_set_geometry")) return rc;
+    if (!tag || !bc) return set_error(LB_ERR_ARG, "lbgpu_set_geometry: null tag or table");
+    Lattice &L = h->L;
+    std::vector<int> src;
+    bool any = false;
+    zgb_slots_from_rows(L, zgb_row, src, any);
+    if (any && L.lx < 2) return set_error(LB_ERR_ARG, "extrapolated outlet needs lx >= 2");
+    if (int rc = L.upload_tags(tag)) return rc;
+    if (int rc = L.upload_bc(bc)) return rc;
+    if (int rc = L.upload_zgb_src(src.data())) return rc;
+    L.zgb_each_step = any;
+    L.d.omega = omega;
+    return LB_OK;
+}
+
+int lbgpu_set_offset_scale(lbgpu_lattice *h, int scale_log2)
+{
+    if (int rc = bad_handle(h, "lbgpu_set_offset_scale")) return rc;
+    if (scale_log2 < -30 || scale_log2 > 30)
+        return set_error(LB_ERR_ARG, "offset scale 2^%d out of range", scale_log2);
+    h->L.d.scale = ldexpf(1.0f, scale_log2);
+    h->L.d.inv_scale = ldexpf(1.0f, -scale_log2);
+    return LB_OK;
+}
+
+int lbgpu_set_populations(lbgpu_lattice *h, const double *f, const double *tmp)
+{
+    if (int rc = bad_handle(h, "lbgpu_set_populations")) return rc;
+    if (!f) return set_error(LB_ERR_ARG, "lbgpu_set_populations: null populations");
+    Lattice &L = h->L;
+    L.launches = 0;
+    if (int rc = L.upload_records(0, f, 9, 0, L.lx + 2)) return rc;
+    if (tmp) {
+        if (int rc = L.upload_records(1, tmp, 9, 0, L.lx + 2)) return rc;
+    } else {
+        if (int rc = lbgpu::cuda_error(cudaMemsetAsync(L.d.buf[1], 0, 9 * (size_t)L.d.g.plane * L.elem,
+                                                       L.stream), "clear second buffer"))
+            return rc;
+    }
+    // the first stream leaves the second buffer's content in the stale slots: side parity 1
+    if (int rc = L.init_side_from(1, 1)) return rc;
+    L.cur = 0; L.form = lbgpu::FORM_L; L.pending = 0; L.n = 0;
+    return lbgpu::cuda_error(cudaStreamSynchronize(L.stream), "lbgpu_set_populations");
+}
+
+int lbgpu_setup_cylinder(lbgpu_lattice *h, int obst_x, int obst_y, int obst_r, double umax,
+                         double re, int wall_kind, int outlet_kind, double *omega_out)
+{
+    if (int rc = bad_handle(h, "lbgpu_setup_cylinder")) return rc;
+    Lattice &L = h->L;
+    const size_t nodes = (size_t)(L.lx + 2) * (L.ly + 2);
+    std::vector<uint8_t> tag(nodes), zgb(L.ly + 2);
+    std::vector<double> bc(16 * (size_t)L.d.g.nb);
+    const double omega = lbgpu_build_cylinder(L.lx, L.ly, obst_x, obst_y, obst_r, umax, re,
+                                              wall_kind, outlet_kind, tag.data(), bc.data(),
+                                              zgb.data(), nullptr);
+    if (omega_out) *omega_out = omega;
+    if (int rc = lbgpu_set_geometry(h, omega, tag.data(), bc.data(), zgb.data())) return rc;
+    L.launches = 0;
+    for (int b = 0; b < 2; ++b)
+        if (L.d.buf[b])
+            if (int rc = lbgpu::cuda_error(cudaMemsetAsync(L.d.buf[b], 0, 9 * (size_t)L.d.g.plane * L.elem,
+                                                           L.stream), "clear populations"))
+                return rc;
+    if (int rc = L.init_cylinder(umax)) return rc;
+    if (int rc = L.init_side_from(1, 1)) return rc;
+    L.cur = 0; L.form = lbgpu::FORM_L; L.pending = 0; L.n = 0;
+    return lbgpu::cuda_error(cudaStreamSynchronize(L.stream), "lbgpu_setup_cylinder");
+}
+
+int lbgpu_step(lbgpu_lattice *h, int nsteps)
+{
+    if (int rc = bad_handle(h, "lbgpu_step")) return rc;
+    return h->L.step(nsteps);
+}
+
+int lbgpu_step_timed(lbgpu_lattice *h, int nsteps, float *ms)
+{
+    if (int rc = bad_handle(h, "lbgpu_step_timed")) return rc;
+    Lattice &L = h->L;
+    cudaEvent_t e0, e1;
+    if (int rc = lbgpu::cuda_error(cudaEventCreate(&e0), "cudaEventCreate")) return rc;
+    if (int rc = lbgpu::cuda_error(cudaEventCreate(&e1), "cudaEventCreate")) {
+        cudaEventDestroy(e0);
+        return rc;
+    }
+    int rc = lbgpu::cuda_error(cudaEventRecord(e0, L.stream), "cudaEventRecord");
+    if (rc == LB_OK) rc = L.step(nsteps);
+    if (rc == LB_OK) rc = lbgpu::cuda_error(cudaEventRecord(e1, L.stream), "cudaEventRecord");
+    if (rc == LB_OK) rc = lbgpu::cuda_error(cudaEventSynchronize(e1), "cudaEventSynchronize");
+    float t = 0.f;
+    if (rc == LB_OK) rc = lbgpu::cuda_error(cudaEventElapsedTime(&t, e0, e1), "cudaEventElapsedTime");
+    if (ms) *ms = t;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
+int lbgpu_get_populations(lbgpu_lattice *h, double *f)
+{
+    if (int rc = bad_handle(h, "lbgpu_get_populations")) return rc;
+    if (!f) return set_error(LB_ERR_ARG, "lbgpu_get_populations: null output");
+    return h->L.readout_records(f, 9, nullptr, 0, h->L.lx + 2);
+}
+
+int lbgpu_get_macros(lbgpu_lattice *h, double *rho, double *ux, double *uy)
+{
+    if (int rc = bad_handle(h, "lbgpu_get_macros")) return rc;
+    return h->L.get_macros(rho, ux, uy);
+}
+
+int lbgpu_synchronize(lbgpu_lattice *h)
+{
+    if (int rc = bad_handle(h, "lbgpu_synchronize")) return rc;
+    return lbgpu::cuda_error(cudaStreamSynchronize(h->L.stream), "lbgpu_synchronize");
+}
+
+void *lbgpu_stream(lbgpu_lattice *h) { return h ? (void *)h->L.stream : nullptr; }
+long long lbgpu_steps_done(lbgpu_lattice *h)
+{
+    if (!h) return 0;
+    return h->L.n + ((h->L.form == lbgpu::FORM_C && h->L.pending) ? 1 : 0);
+}
+size_t lbgpu_device_bytes(lbgpu_lattice *h) { return h ? h->L.bytes : 0; }
+int lbgpu_last_kernel_launches(lbgpu_lattice *h) { return h ? h->L.launches : 0; }
+
+}  // extern "C"

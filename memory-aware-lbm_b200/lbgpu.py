@@ -1,0 +1,261 @@
+"""ctypes binding of liblbgpu.so (include/lb.h, include/lbgpu.h, include/lbdriver.h).
+
+Host-side plumbing for tests and benchmarks: every call goes through the library's C ABI and
+every step runs the library's sm_100a kernels.  There is no Python or CPU fallback; if the
+shared library is missing, importing its functions raises.
+
+Arrays use the reference's node order: f[X, Y, i] for X = 0..lx+1, Y = 0..ly+1 (ghost ring
+included), direction order of the reference (lb.c:48-55).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "liblbgpu.so")
+INCLUDE_DIR = os.path.join(os.path.dirname(HERE), "include")
+
+PRECISIONS = {"f64": 0, "f32": 1, "f16": 2, "bf16": 3}
+SCHEMES = {"pull": 0, "aa": 1}
+BYTES_PER_UPDATE = {"f64": 144, "f32": 72, "f16": 36, "bf16": 36}
+WALL_REGULARIZED, WALL_BOUNCEBACK = 0, 1
+OUTLET_ZGB, OUTLET_CONST = 0, 1
+VARIANTS = {"origin": 0, "combine": 1, "tight": 2, "tight_block": 3, "panel": 4}
+SYNC = {"none": 0, "outlet": 1, "full": 2}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_vp = ctypes.c_void_p
+
+
+class LbError(RuntimeError):
+    """A library call returned an LB_ERR_* code."""
+
+    def __init__(self, code, message):
+        super().__init__(f"liblbgpu error {code}: {message}")
+        self.code = code
+
+
+class DriverConfig(ctypes.Structure):
+    _fields_ = [("lx", ctypes.c_int), ("ly", ctypes.c_int), ("obst_x", ctypes.c_int),
+                ("obst_y", ctypes.c_int), ("obst_r", ctypes.c_int), ("umax", ctypes.c_double),
+                ("re", ctypes.c_double), ("wall", ctypes.c_int), ("outlet", ctypes.c_int),
+                ("variant", ctypes.c_int), ("blk", ctypes.c_int), ("sync_mode", ctypes.c_int)]
+
+
+_LIB = None
+
+
+def lib():
+    """Load liblbgpu.so (raises FileNotFoundError when it is not built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} is not built: run `make -C memory-aware-lbm_b200`")
+    L = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
+    L.lbGetLastError.restype = ctypes.c_int
+    L.lbGetLastErrorString.restype = ctypes.c_char_p
+    L.lbgpu_create.argtypes = [ctypes.c_int] * 4 + [ctypes.POINTER(_vp)]
+    L.lbgpu_destroy.argtypes = [_vp]
+    L.lbgpu_set_geometry.argtypes = [_vp, ctypes.c_double, _u8p, _dp, _u8p]
+    L.lbgpu_set_populations.argtypes = [_vp, _dp, _dp]
+    L.lbgpu_set_offset_scale.argtypes = [_vp, ctypes.c_int]
+    L.lbgpu_setup_cylinder.argtypes = [_vp] + [ctypes.c_int] * 3 + [ctypes.c_double] * 2 + [
+        ctypes.c_int] * 2 + [_dp]
+    L.lbgpu_build_cylinder.restype = ctypes.c_double
+    L.lbgpu_build_cylinder.argtypes = [ctypes.c_int] * 5 + [ctypes.c_double] * 2 + [
+        ctypes.c_int] * 2 + [_u8p, _dp, _u8p, _dp]
+    L.lbgpu_step.argtypes = [_vp, ctypes.c_int]
+    L.lbgpu_step_timed.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    L.lbgpu_get_populations.argtypes = [_vp, _dp]
+    L.lbgpu_get_macros.argtypes = [_vp, _dp, _dp, _dp]
+    L.lbgpu_synchronize.argtypes = [_vp]
+    L.lbgpu_stream.restype = _vp
+    L.lbgpu_stream.argtypes = [_vp]
+    L.lbgpu_steps_done.restype = ctypes.c_longlong
+    L.lbgpu_steps_done.argtypes = [_vp]
+    L.lbgpu_device_bytes.restype = ctypes.c_size_t
+    L.lbgpu_device_bytes.argtypes = [_vp]
+    L.lbgpu_last_kernel_launches.argtypes = [_vp]
+    L.lbdrv_run.argtypes = [ctypes.POINTER(DriverConfig), ctypes.c_int, _dp,
+                            ctypes.POINTER(ctypes.c_double)]
+    L.computeMacros.argtypes = [_dp, _dp, _dp, _dp]
+    L.computeEquilibrium.restype = ctypes.c_double
+    L.computeEquilibrium.argtypes = [ctypes.c_int] + [ctypes.c_double] * 4
+    _LIB = L
+    return L
+
+
+def last_error():
+    L = lib()
+    return L.lbGetLastError(), (L.lbGetLastErrorString() or b"").decode()
+
+
+def clear_error():
+    lib().lbClearError()
+
+
+def _check(rc):
+    if rc != 0:
+        code, msg = last_error()
+        clear_error()
+        raise LbError(rc, msg)
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def build_cylinder(lx, ly, obst_x, obst_y, obst_r, umax=0.02, re=100.0, wall=WALL_REGULARIZED,
+                   outlet=OUTLET_ZGB, populations=True):
+    """Host arrays of the cylinder channel: (omega, tag[X,Y], bc, zgb_row, f[X,Y,9] or None)."""
+    n2 = (lx + 2) * (ly + 2)
+    nb = max(lx, ly) + 2
+    tag = np.zeros(n2, np.uint8)
+    bc = np.zeros(16 * nb)
+    zgb = np.zeros(ly + 2, np.uint8)
+    f = np.zeros(n2 * 9) if populations else None
+    omega = lib().lbgpu_build_cylinder(lx, ly, obst_x, obst_y, obst_r, umax, re, wall, outlet,
+                                       _p(tag, _u8p), _p(bc), _p(zgb, _u8p),
+                                       _p(f) if f is not None else None)
+    return (omega, tag.reshape(lx + 2, ly + 2), bc, zgb,
+            f.reshape(lx + 2, ly + 2, 9) if f is not None else None)
+
+
+class Lattice:
+    """A device lattice (lbgpu_lattice): FP64/FP32/FP16/BF16 storage, pull or AA kernel."""
+
+    def __init__(self, lx, ly, precision="f64", scheme="pull"):
+        self.lx, self.ly, self.precision, self.scheme = lx, ly, precision, scheme
+        h = _vp()
+        _check(lib().lbgpu_create(lx, ly, PRECISIONS[precision], SCHEMES[scheme], ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().lbgpu_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_geometry(self, omega, tag, bc, zgb=None):
+        tag = np.ascontiguousarray(tag, np.uint8).reshape(-1)
+        bc = np.ascontiguousarray(bc, np.float64).reshape(-1)
+        z = None if zgb is None else np.ascontiguousarray(zgb, np.uint8)
+        _check(lib().lbgpu_set_geometry(self.h, float(omega), _p(tag, _u8p), _p(bc),
+                                        None if z is None else _p(z, _u8p)))
+
+    def set_populations(self, f, tmp=None):
+        f = np.ascontiguousarray(f, np.float64).reshape(-1)
+        t = None if tmp is None else np.ascontiguousarray(tmp, np.float64).reshape(-1)
+        _check(lib().lbgpu_set_populations(self.h, _p(f), None if t is None else _p(t)))
+
+    def set_offset_scale(self, scale_log2):
+        _check(lib().lbgpu_set_offset_scale(self.h, int(scale_log2)))
+
+    def setup_cylinder(self, obst_x, obst_y, obst_r, umax=0.02, re=100.0, wall=WALL_REGULARIZED,
+                       outlet=OUTLET_ZGB):
+        om = ctypes.c_double()
+        _check(lib().lbgpu_setup_cylinder(self.h, obst_x, obst_y, obst_r, umax, re, wall, outlet,
+                                          ctypes.byref(om)))
+        return om.value
+
+    def step(self, n):
+        _check(lib().lbgpu_step(self.h, int(n)))
+
+    def step_timed(self, n):
+        ms = ctypes.c_float()
+        _check(lib().lbgpu_step_timed(self.h, int(n), ctypes.byref(ms)))
+        return ms.value
+
+    def synchronize(self):
+        _check(lib().lbgpu_synchronize(self.h))
+
+    def populations(self):
+        out = np.zeros((self.lx + 2) * (self.ly + 2) * 9)
+        _check(lib().lbgpu_get_populations(self.h, _p(out)))
+        return out.reshape(self.lx + 2, self.ly + 2, 9)
+
+    def macros(self):
+        n = self.lx * self.ly
+        rho, ux, uy = np.zeros(n), np.zeros(n), np.zeros(n)
+        _check(lib().lbgpu_get_macros(self.h, _p(rho), _p(ux), _p(uy)))
+        shp = (self.ly, self.lx)
+        return rho.reshape(shp), ux.reshape(shp), uy.reshape(shp)
+
+    @property
+    def stream(self):
+        return lib().lbgpu_stream(self.h)
+
+    @property
+    def steps_done(self):
+        return lib().lbgpu_steps_done(self.h)
+
+    @property
+    def device_bytes(self):
+        return lib().lbgpu_device_bytes(self.h)
+
+    @property
+    def last_launches(self):
+        return lib().lbgpu_last_kernel_launches(self.h)
+
+
+def cylinder_lattice(lx, ly, precision="f64", scheme="pull", umax=0.02, re=100.0,
+                     wall=WALL_BOUNCEBACK, outlet=OUTLET_CONST, obst=None):
+    """A device lattice holding the channel (obstacle default (lx/5+1, ly/2+1), r = ly/10+1)."""
+    ox, oy, r = obst if obst is not None else (lx // 5 + 1, ly // 2 + 1, ly // 10 + 1)
+    lat = Lattice(lx, ly, precision, scheme)
+    lat.omega = lat.setup_cylinder(ox, oy, r, umax, re, wall, outlet)
+    return lat
+
+
+def drive(lx, ly, obst_x, obst_y, obst_r, nsteps, variant="origin", umax=0.02, re=100.0,
+          wall=WALL_REGULARIZED, outlet=OUTLET_ZGB, blk=1, sync="outlet", want_lattice=True):
+    """Run the C host driver (include/lbdriver.h) on the drop-in interface.
+
+    Returns (final lattice f[X,Y,9] or None, steps run, loop wall seconds)."""
+    cfg = DriverConfig(lx, ly, obst_x, obst_y, obst_r, umax, re, wall, outlet, VARIANTS[variant],
+                       blk, SYNC[sync] if isinstance(sync, str) else int(sync))
+    out = np.zeros((lx + 2) * (ly + 2) * 9) if want_lattice else None
+    secs = ctypes.c_double()
+    done = lib().lbdrv_run(ctypes.byref(cfg), int(nsteps), None if out is None else _p(out),
+                           ctypes.byref(secs))
+    if done < 0:
+        code, msg = last_error()
+        clear_error()
+        raise LbError(-done, msg)
+    return (out.reshape(lx + 2, ly + 2, 9) if out is not None else None), done, secs.value
+
+
+def declared_functions():
+    """Names of the functions declared in include/*.h (the C ABI this library exports)."""
+    import re
+    names = set()
+    pat = re.compile(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_ ]*[\s\*]+([A-Za-z_][A-Za-z0-9_]*)\s*\(")
+    for fn in sorted(os.listdir(INCLUDE_DIR)):
+        if not fn.endswith(".h"):
+            continue
+        with open(os.path.join(INCLUDE_DIR, fn)) as fh:
+            text = fh.read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for line in text.splitlines():
+            if line.strip().startswith(("#", "typedef", "//", "return")):
+                continue
+            m = pat.match(line)
+            if m and m.group(1) not in ("if", "for", "while", "switch"):
+                names.add(m.group(1))
+    return sorted(names)
