@@ -93,6 +93,12 @@ enum { LBGPU_OUTLET_ZGB = 0, LBGPU_OUTLET_CONST = 1 };
 
 typedef struct lbgpu_lattice lbgpu_lattice;
 
+/* Select the CUDA device used by this thread's later lbgpu_create / constructSim calls (the
+ * library carries its own CUDA runtime, so a device chosen through another runtime, such as
+ * the one PyTorch loads, does not carry over).  Returns LB_ERR_NO_DEVICE for a bad index. */
+int lbgpu_set_device(int device);
+int lbgpu_device_count(void);
+
 /* Allocate a lattice on the current CUDA device: two population buffers for
  * LBGPU_PULL, one for LBGPU_AA, plus tags and tables. */
 int lbgpu_create(int lx, int ly, int precision, int scheme, lbgpu_lattice **out);

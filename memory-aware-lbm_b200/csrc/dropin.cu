@@ -219,6 +219,21 @@ void pin_host(Simulation *sim, DropIn *c)
     }
 }
 
+// Create the device lattice and pin the host arrays (once).
+int create_device(Simulation *sim, DropIn *c)
+{
+    if (c->created) return LB_OK;
+    Lattice &L = c->L;
+    if (int rc = L.create(sim->lx, sim->ly, LBGPU_F64, LBGPU_PULL)) {
+        L.destroy();
+        return rc;
+    }
+    L.ghosts = true;
+    c->created = true;
+    pin_host(sim, c);
+    return LB_OK;
+}
+
 // Bring the device copy up to date before an entry point runs.
 DropIn *prepare(Simulation *sim, const char *fn)
 {
@@ -228,15 +243,7 @@ DropIn *prepare(Simulation *sim, const char *fn)
         return nullptr;
     }
     Lattice &L = c->L;
-    if (!c->created) {
-        if (L.create(sim->lx, sim->ly, LBGPU_F64, LBGPU_PULL) != LB_OK) {
-            L.destroy();
-            return nullptr;
-        }
-        L.ghosts = true;
-        c->created = true;
-        pin_host(sim, c);
-    }
+    if (!c->created && create_device(sim, c) != LB_OK) return nullptr;
     if (c->tags_dirty) {
         if (scan_dynamics(sim, c) != LB_OK) return nullptr;
         c->tags_dirty = false;
@@ -400,6 +407,12 @@ void constructSim(Simulation *sim, int lx, int ly)
         else c->sync_mode = LB_SYNC_OUTLET;
     }
     sim->device = c;
+    // Allocate the device lattice and pin the host arrays now, as part of construction (the
+    // reference's drivers time the steps only).  Without a usable device this is retried at
+    // the first step, where a failure is reported.
+    if (lbgpu::last_error() == LB_OK && lbgpu_device_count() > 0) {
+        if (create_device(sim, c) != LB_OK) lbgpu::clear_error();
+    }
 }
 
 void destructSim(Simulation *sim)

@@ -65,6 +65,9 @@ int Lattice::create(int lx_, int ly_, int precision_, int scheme_)
         return set_error(LB_ERR_ARG, "unknown precision %d", precision_);
     if (scheme_ != LBGPU_PULL && scheme_ != LBGPU_AA)
         return set_error(LB_ERR_ARG, "unknown scheme %d", scheme_);
+    if (precision_ != LBGPU_F64 || scheme_ != LBGPU_PULL)
+        return set_error(LB_ERR_ARG, "precision %d / scheme %d kernels are not built", precision_,
+                         scheme_);
     lx = lx_; ly = ly_; precision = precision_; scheme = scheme_;
     elem = elem_bytes(precision);
     d.g = make_geo(lx, ly, (int)elem);

@@ -42,6 +42,25 @@ int lbGetLastError(void) { return lbgpu::last_error(); }
 const char *lbGetLastErrorString(void) { return lbgpu::last_error_string(); }
 void lbClearError(void) { lbgpu::clear_error(); }
 
+int lbgpu_set_device(int device)
+{
+    int n = 0;
+    if (int rc = lbgpu::cuda_error(cudaGetDeviceCount(&n), "cudaGetDeviceCount")) return rc;
+    if (device < 0 || device >= n)
+        return set_error(LB_ERR_NO_DEVICE, "device %d requested, %d present", device, n);
+    return lbgpu::cuda_error(cudaSetDevice(device), "cudaSetDevice");
+}
+
+int lbgpu_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
 int lbgpu_create(int lx, int ly, int precision, int scheme, lbgpu_lattice **out)
 {
     if (!out) return set_error(LB_ERR_ARG, "lbgpu_create: null output pointer");

@@ -56,9 +56,13 @@ def lib():
         return _LIB
     if not os.path.exists(LIB_PATH):
         raise FileNotFoundError(f"{LIB_PATH} is not built: run `make -C memory-aware-lbm_b200`")
-    L = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
+    # RTLD_LOCAL: the library exports the reference's symbol names (collide, bgk, ...); they must
+    # not take the place of the reference's own definitions in libraries loaded later
+    L = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_LOCAL)
     L.lbGetLastError.restype = ctypes.c_int
     L.lbGetLastErrorString.restype = ctypes.c_char_p
+    L.lbgpu_set_device.argtypes = [ctypes.c_int]
+    L.lbgpu_device_count.restype = ctypes.c_int
     L.lbgpu_create.argtypes = [ctypes.c_int] * 4 + [ctypes.POINTER(_vp)]
     L.lbgpu_destroy.argtypes = [_vp]
     L.lbgpu_set_geometry.argtypes = [_vp, ctypes.c_double, _u8p, _dp, _u8p]
