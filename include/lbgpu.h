@@ -143,6 +143,16 @@ int lbgpu_get_populations(lbgpu_lattice *lat, double *f);
  * (ly rows of lx values), computed on the device. Any pointer may be NULL. */
 int lbgpu_get_macros(lbgpu_lattice *lat, double *rho, double *ux, double *uy);
 
+/* lbgpu_get_macros for callers that cannot allocate device memory while the solver runs (a
+ * serving loop reading one simulation while others step: cudaMalloc/cudaFree would stall every
+ * stream; a process whose device memory another allocator has reserved).  No counterpart in
+ * the reference.  Allocates nothing: the device scratch is a fixed array of 3 x 262,144
+ * doubles (6 MiB, held by every GPU that loads the library), so lattices above 262,144
+ * interior nodes get LB_ERR_CAPACITY.  The first call on a device looks up that array's
+ * address; make it before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race. */
+int lbgpu_get_macros_noalloc(lbgpu_lattice *lat, double *rho, double *ux, double *uy);
+
 int lbgpu_synchronize(lbgpu_lattice *lat);
 void *lbgpu_stream(lbgpu_lattice *lat);           /* the lattice's cudaStream_t            */
 long long lbgpu_steps_done(lbgpu_lattice *lat);

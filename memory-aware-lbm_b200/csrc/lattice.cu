@@ -76,6 +76,7 @@ int Lattice::create(int lx_, int ly_, int precision_, int scheme_)
     int ndev = 0;
     LB_CUDA(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
     if (ndev == 0) return set_error(LB_ERR_NO_DEVICE, "no CUDA device");
+    LB_CUDA(cudaGetDevice(&device), "cudaGetDevice");
     LB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
 
     const size_t nbuf = (scheme == LBGPU_AA) ? 1 : 2;

@@ -32,6 +32,7 @@ struct Lattice {
     cudaStream_t stream = nullptr;
     size_t bytes = 0;
     int launches = 0;    // kernels launched by the last public call
+    int device = 0;      // CUDA device the lattice lives on
 
     std::vector<double> bc_host;   // [16*nb] last uploaded boundary tables
     std::vector<int> zgb_src_host; // [4*nb]
@@ -65,3 +66,8 @@ struct Lattice {
 };
 
 }  // namespace lbgpu
+
+// The opaque handle of include/lbgpu.h.
+struct lbgpu_lattice {
+    lbgpu::Lattice L;
+};

@@ -7,10 +7,6 @@
 using lbgpu::Lattice;
 using lbgpu::set_error;
 
-struct lbgpu_lattice {
-    Lattice L;
-};
-
 namespace {
 
 int bad_handle(const lbgpu_lattice *h, const char *fn)

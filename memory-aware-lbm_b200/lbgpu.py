@@ -77,6 +77,7 @@ def lib():
     L.lbgpu_step_timed.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     L.lbgpu_get_populations.argtypes = [_vp, _dp]
     L.lbgpu_get_macros.argtypes = [_vp, _dp, _dp, _dp]
+    L.lbgpu_get_macros_noalloc.argtypes = [_vp, _dp, _dp, _dp]
     L.lbgpu_synchronize.argtypes = [_vp]
     L.lbgpu_stream.restype = _vp
     L.lbgpu_stream.argtypes = [_vp]
@@ -198,6 +199,14 @@ class Lattice:
         n = self.lx * self.ly
         rho, ux, uy = np.zeros(n), np.zeros(n), np.zeros(n)
         _check(lib().lbgpu_get_macros(self.h, _p(rho), _p(ux), _p(uy)))
+        shp = (self.ly, self.lx)
+        return rho.reshape(shp), ux.reshape(shp), uy.reshape(shp)
+
+    def macros_noalloc(self):
+        """lbgpu_get_macros_noalloc: the same read-out through the library's fixed scratch."""
+        n = self.lx * self.ly
+        rho, ux, uy = np.zeros(n), np.zeros(n), np.zeros(n)
+        _check(lib().lbgpu_get_macros_noalloc(self.h, _p(rho), _p(ux), _p(uy)))
         shp = (self.ly, self.lx)
         return rho.reshape(shp), ux.reshape(shp), uy.reshape(shp)
 

@@ -1,0 +1,73 @@
+"""lbgpu_get_macros_noalloc: the density/velocity read-out for callers that cannot allocate.
+
+Such callers (a serving loop reading one simulation while others keep stepping, where
+cudaMalloc/cudaFree would stall every stream; a process whose device memory another allocator
+has reserved) get the same numbers as lbgpu_get_macros from a fixed device array.  The check is
+against the allocating entry point with the tolerance of the FP64 parity tests, which is zero:
+both run the same kernel on the same state, so the results must be bit-identical -- on two calls
+in a row, so the second call sees the array the first one left behind.
+
+This file is collected last so a stop-at-first-failure run has run every other test first; it
+also passes alone in a fresh process (the first call on the device does the scratch set-up).
+"""
+import numpy as np
+import pytest
+
+import lbgpu
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+LB_ERR_CAPACITY = 10
+
+
+def _bits(a):
+    return np.ascontiguousarray(a).view(np.uint64)
+
+
+def _lattice(c, steps):
+    st = O.build_cylinder(c)
+    lat = lbgpu.Lattice(c.lx, c.ly, "f64", "pull")
+    lat.set_geometry(st.omega, st.tag, st.bc, st.zgb)
+    lat.set_populations(st.lat, st.tmp)
+    lat.step(steps)
+    return lat
+
+
+def test_noalloc_readout_matches_allocating_readout_on_two_calls_in_a_row():
+    with _lattice(O.Cylinder.baseline(250, 51), 40) as lat:
+        want = lat.macros()
+        first = lat.macros_noalloc()
+        second = lat.macros_noalloc()
+    for w, a, b in zip(want, first, second):
+        assert np.array_equal(_bits(w), _bits(a))
+        assert np.array_equal(_bits(w), _bits(b))
+
+
+def test_noalloc_readout_after_another_lattice_used_the_scratch():
+    # a larger lattice fills more of the shared array; the next, smaller read-out must not
+    # see any of it
+    with _lattice(O.Cylinder.reference_driver(480, 300), 25) as big:
+        big_want = big.macros()
+        big_got = big.macros_noalloc()
+    for w, g in zip(big_want, big_got):
+        assert np.array_equal(_bits(w), _bits(g))
+    with _lattice(O.Cylinder.baseline(64, 33), 10) as small:
+        want = small.macros()
+        a = small.macros_noalloc()
+        b = small.macros_noalloc()
+    for w, x, y in zip(want, a, b):
+        assert np.array_equal(_bits(w), _bits(x))
+        assert np.array_equal(_bits(w), _bits(y))
+
+
+def test_noalloc_rejects_lattices_beyond_the_fixed_scratch():
+    with lbgpu.Lattice(1024, 512, "f64", "pull") as lat:   # 524,288 nodes > 262,144
+        lat.setup_cylinder(205, 257, 52, 0.02, 100.0, lbgpu.WALL_BOUNCEBACK, lbgpu.OUTLET_CONST)
+        with pytest.raises(lbgpu.LbError) as e:
+            lat.macros_noalloc()
+        assert e.value.code == LB_ERR_CAPACITY
+        assert "262144" in str(e.value)
+        # the allocating entry point still serves it
+        rho, _, _ = lat.macros()
+        assert rho.shape == (512, 1024) and np.isfinite(rho).all()
