@@ -554,7 +554,7 @@ void makePeriodic(Simulation *sim)
     L.launches = 0;
     c->tmp_is_stream = false;
     if (L.materialize()) return;
-    lbgpu::launch_periodic_f64(L.d, L.cur, L.stream);
+    lbgpu::launch_periodic(L.d, L.cur, L.stream);
     ++L.launches;
     if (L.form == lbgpu::FORM_C) {
         // the wrap rewrote stale slots of a collided state: refresh their record

@@ -1,0 +1,575 @@
+// kernels.cu -- step, read-out and set-up kernels for sm_100a, for every storage type.
+//
+// State convention shared by every kernel here (n = index of the last collision):
+//   pull form L : buffer `cur` holds the post-stream populations L_m, stale slots included.
+//   pull form C : buffer `cur` holds the post-collision populations C_n; the post-stream state
+//                 L_{n+1} is "C_n streamed", read through logical().
+//   AA natural  : the AA buffer holds L_m in each node's own slots (stale slots in the side store).
+//   AA swapped  : the AA buffer holds C_n of direction i in slot opp(i) of each node.
+//   side store parity p = k & 1 holds the post-collision values C_k of the perimeter nodes'
+//   stale slots, which the stream two steps later must leave in place (reference: in-place
+//   collision lb.c:181-185 + propagation that never reads ghost sources lb.c:258-267 into a
+//   second buffer that is reused every other step).
+//
+// Storage types: double (exact FP64 arithmetic), float, __half / __nv_bfloat16 offsets
+// (codec.cuh), all with the same index space (layout.cuh).
+#include "codec.cuh"
+#include "kernels.h"
+#include "lbgpu.h"
+
+namespace lbgpu {
+
+namespace {
+
+constexpr int BX = 128;  // threads along x per block (coalesced axis)
+
+template <class S>
+__device__ __forceinline__ const S *plane(const S *b, const Geo &g, int i)
+{
+    return b + (size_t)i * (size_t)g.plane;
+}
+template <class S>
+__device__ __forceinline__ S *plane(S *b, const Geo &g, int i)
+{
+    return b + (size_t)i * (size_t)g.plane;
+}
+
+// Table entry (p0, p1) of a boundary node: (ux, uy) or (rho, uPar).
+__device__ __forceinline__ void node_params(const double *__restrict__ bc, const Geo &g, int t,
+                                            int X, int Y, double &p0, double &p1)
+{
+    p0 = 0.0; p1 = 0.0;
+    if (t >= TAG_ZOUHE_FIRST && t < TAG_COUNT) {
+        const int tb = tag_table(t);
+        const int coord = (tag_side(t) <= SIDE_LOWER) ? X : Y;
+        p0 = bc[(tb * 2 + 0) * g.nb + coord];
+        p1 = bc[(tb * 2 + 1) * g.nb + coord];
+    }
+}
+
+template <class S>
+__device__ __forceinline__ void collide_node(const double *__restrict__ bc, const Geo &g, int t,
+                                             int X, int Y, typename Codec<S>::R f[9], double omega)
+{
+    using R = typename Codec<S>::R;
+    double p0, p1;
+    node_params(bc, g, t, X, Y, p0, p1);
+    rules::collide<R>(t, f, (R)omega, (R)p0, (R)p1);
+}
+
+// Post-stream value of slot i at node (X, Y), any node of the lattice including the ghost
+// ring, under each view (kernels.h).  Ghost slots that no interior node streams into keep the
+// content of the buffer the state lives in, as in the reference: for the pull scheme `other`
+// is the second buffer; for the AA scheme's swapped view (an odd step count, which the
+// reference leaves in its second buffer) `other` is that buffer's saved ghost ring
+// [9][nghost].
+template <class S>
+__device__ __forceinline__ typename Codec<S>::R logical(const Geo &g, int view, const S *__restrict__ cur,
+                                                        const S *__restrict__ other,
+                                                        const S *__restrict__ side, int X, int Y,
+                                                        int i, float inv)
+{
+    using C = Codec<S>;
+    const int sx = X - cx(i), sy = Y - cy(i);
+    switch (view) {
+    case VIEW_PULL_PENDING:
+        if (g.interior(sx, sy)) return C::dec(plane(cur, g, i)[g.idx(sx, sy)], i, inv);
+        if (g.interior(X, Y)) return C::dec(side[(size_t)i * g.nper + g.pidx(X, Y)], i, inv);
+        return C::dec(plane(other, g, i)[g.idx(X, Y)], i, inv);
+    case VIEW_AA_NATURAL:
+        if (g.interior(X, Y) && !g.interior(sx, sy))
+            return C::dec(side[(size_t)i * g.nper + g.pidx(X, Y)], i, inv);
+        return C::dec(plane(cur, g, i)[g.idx(X, Y)], i, inv);
+    case VIEW_AA_SWAPPED:
+        if (g.interior(sx, sy)) return C::dec(plane(cur, g, opp(i))[g.idx(sx, sy)], i, inv);
+        if (g.interior(X, Y)) return C::dec(side[(size_t)i * g.nper + g.pidx(X, Y)], i, inv);
+        return C::dec(other[(size_t)i * g.nghost() + g.gidx(X, Y)], i, inv);
+    default:
+        return C::dec(plane(cur, g, i)[g.idx(X, Y)], i, inv);
+    }
+}
+
+// ---- pull scheme --------------------------------------------------------------------------
+
+// In-place collision of every interior node (form L -> form C); the perimeter nodes also
+// record their stale slots' post-collision values in the side parity given.
+template <class S>
+__global__ void __launch_bounds__(BX) k_collide_inplace(Geo g, S *__restrict__ buf,
+                                                        const uint8_t *__restrict__ tag,
+                                                        const double *__restrict__ bc, double omega,
+                                                        S *__restrict__ side, float sc, float inv)
+{
+    using C = Codec<S>;
+    using R = typename C::R;
+    const int X = blockIdx.x * BX + threadIdx.x + 1;
+    const int Y = blockIdx.y + 1;
+    if (X > g.lx) return;
+    const long long o = g.idx(X, Y);
+    R f[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) f[i] = C::dec(plane(buf, g, i)[o], i, inv);
+    collide_node<S>(bc, g, tag[o], X, Y, f, omega);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) plane(buf, g, i)[o] = C::enc(f[i], i, sc);
+    if (g.perimeter(X, Y)) {
+        const int p = g.pidx(X, Y);
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = C::enc(f[i], i, sc);
+    }
+}
+
+// Fused stream + collide (form C_n in `src` -> form C_{n+1} in `dst`): each interior node
+// gathers L_{n+1} from its neighbours (stale slots from the side parity holding C_{n-1}),
+// collides, writes C_{n+1} and refreshes the same side parity.  With GHOSTS, ghost-ring nodes
+// of `dst` receive the values streamed out of the lattice, as the reference's propagation
+// writes them (lb.c:258-267).
+template <class S, bool GHOSTS>
+__global__ void __launch_bounds__(BX) k_pull(Geo g, const S *__restrict__ src, S *__restrict__ dst,
+                                             const uint8_t *__restrict__ tag,
+                                             const double *__restrict__ bc, double omega,
+                                             S *__restrict__ side, float sc, float inv)
+{
+    using C = Codec<S>;
+    using R = typename C::R;
+    const int X = blockIdx.x * BX + threadIdx.x + (GHOSTS ? 0 : 1);
+    const int Y = blockIdx.y + (GHOSTS ? 0 : 1);
+    if (X > g.lx + (GHOSTS ? 1 : 0)) return;
+    const long long o = g.idx(X, Y);
+    if (GHOSTS && !g.interior(X, Y)) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const int sx = X - cx(i), sy = Y - cy(i);
+            if (g.interior(sx, sy)) plane(dst, g, i)[o] = plane(src, g, i)[g.idx(sx, sy)];
+        }
+        return;
+    }
+    R f[9];
+    const bool edge = g.perimeter(X, Y);
+    if (!edge) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            f[i] = C::dec(plane(src, g, i)[o - cx(i) - (long long)cy(i) * g.pitch], i, inv);
+    } else {
+        const int p = g.pidx(X, Y);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const int sx = X - cx(i), sy = Y - cy(i);
+            f[i] = C::dec(g.interior(sx, sy) ? plane(src, g, i)[g.idx(sx, sy)]
+                                             : side[(size_t)i * g.nper + p], i, inv);
+        }
+    }
+    collide_node<S>(bc, g, tag[o], X, Y, f, omega);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = C::enc(f[i], i, sc);
+    if (edge) {
+        const int p = g.pidx(X, Y);
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = C::enc(f[i], i, sc);
+    }
+}
+
+// Propagation of C_n in `src` into `dst` (form C -> form L), ghost ring included; stale
+// slots of interior nodes come from the side parity holding C_{n-1}; ghost slots with no
+// source keep `dst`'s content (lb.c:258-267).  Stored values move unchanged.
+template <class S>
+__global__ void __launch_bounds__(BX) k_stream(Geo g, const S *__restrict__ src, S *__restrict__ dst,
+                                               const S *__restrict__ side)
+{
+    const int X = blockIdx.x * BX + threadIdx.x;
+    const int Y = blockIdx.y;
+    if (X > g.lx + 1) return;
+    const long long o = g.idx(X, Y);
+    const bool in = g.interior(X, Y);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const int sx = X - cx(i), sy = Y - cy(i);
+        if (g.interior(sx, sy)) plane(dst, g, i)[o] = plane(src, g, i)[g.idx(sx, sy)];
+        else if (in) plane(dst, g, i)[o] = side[(size_t)i * g.nper + g.pidx(X, Y)];
+    }
+}
+
+// ---- AA scheme ----------------------------------------------------------------------------
+
+// Even step: own natural slots (stale ones from the side store) -> collide -> own opposite slots.
+template <class S>
+__global__ void __launch_bounds__(BX) k_aa_even(Geo g, S *__restrict__ a,
+                                                const uint8_t *__restrict__ tag,
+                                                const double *__restrict__ bc, double omega,
+                                                S *__restrict__ side, float sc, float inv)
+{
+    using C = Codec<S>;
+    using R = typename C::R;
+    const int X = blockIdx.x * BX + threadIdx.x + 1;
+    const int Y = blockIdx.y + 1;
+    if (X > g.lx) return;
+    const long long o = g.idx(X, Y);
+    const bool edge = g.perimeter(X, Y);
+    const int p = edge ? g.pidx(X, Y) : 0;
+    R f[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const bool stale = edge && !g.interior(X - cx(i), Y - cy(i));
+        f[i] = C::dec(stale ? side[(size_t)i * g.nper + p] : plane(a, g, i)[o], i, inv);
+    }
+    collide_node<S>(bc, g, tag[o], X, Y, f, omega);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) plane(a, g, opp(i))[o] = C::enc(f[i], i, sc);
+    if (edge) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = C::enc(f[i], i, sc);
+    }
+}
+
+// Odd step: gather direction i from the source neighbour's opposite slot (stale slots from the
+// side store) -> collide -> scatter direction i to the destination neighbour's natural slot.
+// Slot A[i][x + c_i] is read (as opp of the neighbour's gather) and written by the same thread,
+// so the in-place update is race-free.  Destinations in the ghost ring are written too, so the
+// natural form carries the values streamed out of the lattice.
+template <class S>
+__global__ void __launch_bounds__(BX) k_aa_odd(Geo g, S *__restrict__ a,
+                                               const uint8_t *__restrict__ tag,
+                                               const double *__restrict__ bc, double omega,
+                                               S *__restrict__ side, float sc, float inv)
+{
+    using C = Codec<S>;
+    using R = typename C::R;
+    const int X = blockIdx.x * BX + threadIdx.x + 1;
+    const int Y = blockIdx.y + 1;
+    if (X > g.lx) return;
+    const long long o = g.idx(X, Y);
+    const bool edge = g.perimeter(X, Y);
+    const int p = edge ? g.pidx(X, Y) : 0;
+    R f[9];
+    if (!edge) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            f[i] = C::dec(plane(a, g, opp(i))[o - cx(i) - (long long)cy(i) * g.pitch], i, inv);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const int sx = X - cx(i), sy = Y - cy(i);
+            f[i] = C::dec(g.interior(sx, sy) ? plane(a, g, opp(i))[g.idx(sx, sy)]
+                                             : side[(size_t)i * g.nper + p], i, inv);
+        }
+    }
+    collide_node<S>(bc, g, tag[o], X, Y, f, omega);
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+        plane(a, g, i)[o + cx(i) + (long long)cy(i) * g.pitch] = C::enc(f[i], i, sc);
+    if (edge) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = C::enc(f[i], i, sc);
+    }
+}
+
+// ---- side store, read-out, upload ----------------------------------------------------------
+
+// Copy the stale slots of the perimeter nodes of buffer b into a side parity.
+template <class S>
+__global__ void k_side_from_buf(Geo g, const S *__restrict__ buf, S *__restrict__ side)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nrow = 2 * g.lx, ncol = g.ly > 2 ? 2 * (g.ly - 2) : 0;
+    if (k >= nrow + ncol) return;
+    int X, Y;
+    if (k < g.lx) { X = k + 1; Y = 1; }
+    else if (k < nrow) { X = k - g.lx + 1; Y = g.ly; }
+    else if (k < nrow + ncol / 2) { X = 1; Y = k - nrow + 2; }
+    else { X = g.lx; Y = k - nrow - ncol / 2 + 2; }
+    const long long o = g.idx(X, Y);
+    const int p = g.pidx(X, Y);
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+        if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = plane(buf, g, i)[o];
+}
+
+// Ghost ring of buffer b into the AA scheme's copy of the second buffer's ring.
+template <class S>
+__global__ void k_ghost_copy(Geo g, const S *__restrict__ buf, S *__restrict__ ring)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ng = g.nghost();
+    if (k >= ng) return;
+    int X, Y;
+    if (k < g.lx + 2) { X = k; Y = 0; }
+    else if (k < 2 * (g.lx + 2)) { X = k - (g.lx + 2); Y = g.ly + 1; }
+    else if (k < 2 * (g.lx + 2) + g.ly) { X = 0; Y = k - 2 * (g.lx + 2) + 1; }
+    else { X = g.lx + 1; Y = k - 2 * (g.lx + 2) - g.ly + 1; }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) ring[(size_t)i * ng + k] = plane(buf, g, i)[g.idx(X, Y)];
+}
+
+// Current state of columns [X0, X1) (all rows) as FP64 node records of `rs` doubles:
+// populations in slots 0..8 and, when `dynp` is given, the host dynamics pointer bits in
+// slot 9 (the host Node layout).
+template <class S>
+__global__ void __launch_bounds__(BX) k_readout(Geo g, int view, const S *__restrict__ cur,
+                                                const S *__restrict__ other,
+                                                const S *__restrict__ side, int X0, int X1,
+                                                double *__restrict__ out, int rs,
+                                                const uint64_t *__restrict__ dynp, float inv)
+{
+    const int Y = blockIdx.x * BX + threadIdx.x;
+    const int X = X0 + blockIdx.y;
+    if (Y > g.ly + 1 || X >= X1) return;
+    const size_t r = ((size_t)(X - X0) * (g.ly + 2) + Y) * rs;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) out[r + i] = (double)logical(g, view, cur, other, side, X, Y, i, inv);
+    if (dynp) out[r + 9] = __longlong_as_double((long long)dynp[(size_t)X * (g.ly + 2) + Y]);
+}
+
+// FP64 node records of columns [X0, X1) into buffer b (inverse of k_readout).
+template <class S>
+__global__ void __launch_bounds__(BX) k_upload(Geo g, const double *__restrict__ in, int rs, int X0,
+                                               int X1, S *__restrict__ buf, float sc)
+{
+    const int Y = blockIdx.x * BX + threadIdx.x;
+    const int X = X0 + blockIdx.y;
+    if (Y > g.ly + 1 || X >= X1) return;
+    const size_t r = ((size_t)(X - X0) * (g.ly + 2) + Y) * rs;
+    const long long o = g.idx(X, Y);
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+        plane(buf, g, i)[o] = Codec<S>::enc((typename Codec<S>::R)in[r + i], i, sc);
+}
+
+// ---- outlet extrapolation, periodic wrap, initial state, macroscopic fields ---------------
+
+// Density of the post-stream state at columns lx-1 and lx-2 for every row (the inputs of the
+// zero-gradient outlet, unsteady.c:205-214 and lb.c:471-480).
+template <class S>
+__global__ void k_zgb_rho(Geo g, int view, const S *__restrict__ cur, const S *__restrict__ other,
+                          const S *__restrict__ side, double *__restrict__ zrho, float inv)
+{
+    using R = typename Codec<S>::R;
+    const int Y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (Y > g.ly + 1) return;
+    R f[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) f[i] = logical(g, view, cur, other, side, g.lx - 1, Y, i, inv);
+    zrho[2 * Y] = (double)rules::density(f);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) f[i] = logical(g, view, cur, other, side, g.lx - 2, Y, i, inv);
+    zrho[2 * Y + 1] = (double)rules::density(f);
+}
+
+// Pressure-table slots fed by the extrapolation: rho = 4/3 rho1 - 1/3 rho2, uPar = 0.
+__global__ void k_zgb_apply(int nb, const int *__restrict__ zgb_src, const double *__restrict__ zrho,
+                            double *__restrict__ bc)
+{
+    using O = Ar<double>;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 4 * nb) return;
+    const int src = zgb_src[k];
+    if (src < 0) return;
+    const int tb = 4 + k / nb, c = k % nb;
+    bc[(tb * 2 + 0) * nb + c] = O::S(O::M(4. / 3., zrho[2 * src]), O::M(1. / 3., zrho[2 * src + 1]));
+    bc[(tb * 2 + 1) * nb + c] = 0.0;
+}
+
+// Periodic wrap of buffer b (pull form L): the slots a boundary node would receive from across
+// the lattice take the values streamed into the opposite ghost ring (lb.c:1783-1817).  The
+// three phases run in the reference's order so that later writes win.
+template <class S>
+__global__ void k_periodic(Geo g, S *__restrict__ buf)
+{
+    const int lx = g.lx, ly = g.ly;
+#define P(i, X, Y) plane(buf, g, (i))[g.idx((X), (Y))]
+    for (int X = 1 + threadIdx.x; X <= lx; X += blockDim.x) {
+        P(4, X, ly) = P(4, X, 0); P(7, X, ly) = P(7, X, 0); P(8, X, ly) = P(8, X, 0);
+        P(2, X, 1) = P(2, X, ly + 1); P(5, X, 1) = P(5, X, ly + 1); P(6, X, 1) = P(6, X, ly + 1);
+    }
+    __syncthreads();
+    for (int Y = 1 + threadIdx.x; Y <= ly; Y += blockDim.x) {
+        P(1, 1, Y) = P(1, lx + 1, Y); P(5, 1, Y) = P(5, lx + 1, Y); P(8, 1, Y) = P(8, lx + 1, Y);
+        P(3, lx, Y) = P(3, 0, Y); P(6, lx, Y) = P(6, 0, Y); P(7, lx, Y) = P(7, 0, Y);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        P(5, 1, 1) = P(5, lx + 1, ly + 1);
+        P(6, lx, 1) = P(6, 0, ly + 1);
+        P(7, lx, ly) = P(7, 0, 0);
+        P(8, 1, ly) = P(8, lx + 1, 0);
+    }
+#undef P
+}
+
+// Equilibrium at rho = 1 and the Poiseuille velocity of row Y, ux = 4 uMax/L^2 (L y - y^2)
+// with y = Y-1, L = ly-1 (unsteady.c:155-159, :169-170), computed in exact FP64 and encoded;
+// ghost ring zero (lb.c:62-68).
+template <class S>
+__global__ void __launch_bounds__(BX) k_init_cylinder(Geo g, S *__restrict__ buf, double umax, float sc)
+{
+    using O = Ar<double>;
+    const int X = blockIdx.x * BX + threadIdx.x;
+    const int Y = blockIdx.y;
+    if (X > g.lx + 1) return;
+    const long long o = g.idx(X, Y);
+    double f[9];
+    if (g.interior(X, Y)) {
+        const double y = (double)(Y - 1), L = (double)(g.ly - 1);
+        const double u = O::M(O::D(O::M(4.0, umax), O::M(L, L)), O::S(O::M(L, y), O::M(y, y)));
+        rules::equilibrium<double>(f, 1.0, u, 0.0);
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            plane(buf, g, i)[o] = Codec<S>::enc((typename Codec<S>::R)f[i], i, sc);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) plane(buf, g, i)[o] = S(0);
+    }
+}
+
+template <class S>
+__global__ void __launch_bounds__(BX) k_macros(Geo g, int view, const S *__restrict__ cur,
+                                               const S *__restrict__ other,
+                                               const S *__restrict__ side, double *__restrict__ rho,
+                                               double *__restrict__ ux, double *__restrict__ uy,
+                                               float inv)
+{
+    using R = typename Codec<S>::R;
+    const int X = blockIdx.x * BX + threadIdx.x + 1;
+    const int Y = blockIdx.y + 1;
+    if (X > g.lx) return;
+    R f[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) f[i] = logical(g, view, cur, other, side, X, Y, i, inv);
+    R r, u, v;
+    rules::macros<R>(f, r, u, v);
+    const size_t k = (size_t)(Y - 1) * g.lx + (X - 1);
+    if (rho) rho[k] = (double)r;
+    if (ux) ux[k] = (double)u;
+    if (uy) uy[k] = (double)v;
+}
+
+inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
+
+template <class S> S *B(const DevLattice &d, int b) { return static_cast<S *>(d.buf[b]); }
+// The `other` argument of logical(): the pull scheme's second buffer, or the AA ring copy.
+template <class S> S *OTHER(const DevLattice &d, int cur)
+{
+    return d.buf[1] ? static_cast<S *>(d.buf[1 - cur]) : static_cast<S *>(d.ghost2);
+}
+template <class S> S *SIDE(const DevLattice &d, int p)
+{
+    return static_cast<S *>(d.side) + (size_t)(p & 1) * 9 * (size_t)d.g.nper;
+}
+
+}  // namespace
+
+// Run F<S>() with S the lattice's storage type.
+#define LBGPU_DISPATCH(d, BODY)                                        \
+    switch ((d).precision) {                                          \
+    case LBGPU_F64: { using S = double; BODY; } break;                \
+    case LBGPU_F32: { using S = float; BODY; } break;                 \
+    case LBGPU_F16: { using S = __half; BODY; } break;                \
+    default: { using S = __nv_bfloat16; BODY; } break;                \
+    }
+
+void launch_collide_inplace(const DevLattice &d, int cur, int side_par, cudaStream_t s)
+{
+    dim3 grid(cdiv(d.g.lx, BX), d.g.ly);
+    LBGPU_DISPATCH(d, (k_collide_inplace<S><<<grid, BX, 0, s>>>(d.g, B<S>(d, cur), d.tag, d.bc,
+                       d.omega, SIDE<S>(d, side_par), d.scale, d.inv_scale)));
+}
+
+void launch_pull(const DevLattice &d, int src, int side_par, bool ghosts, cudaStream_t s)
+{
+    if (ghosts) {
+        dim3 grid(cdiv(d.g.lx + 2, BX), d.g.ly + 2);
+        LBGPU_DISPATCH(d, (k_pull<S, true><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src),
+                           d.tag, d.bc, d.omega, SIDE<S>(d, side_par), d.scale, d.inv_scale)));
+    } else {
+        dim3 grid(cdiv(d.g.lx, BX), d.g.ly);
+        LBGPU_DISPATCH(d, (k_pull<S, false><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src),
+                           d.tag, d.bc, d.omega, SIDE<S>(d, side_par), d.scale, d.inv_scale)));
+    }
+}
+
+void launch_stream(const DevLattice &d, int src, int side_par, cudaStream_t s)
+{
+    dim3 grid(cdiv(d.g.lx + 2, BX), d.g.ly + 2);
+    LBGPU_DISPATCH(d, (k_stream<S><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src),
+                       SIDE<S>(d, side_par))));
+}
+
+void launch_aa_even(const DevLattice &d, int side_par, cudaStream_t s)
+{
+    dim3 grid(cdiv(d.g.lx, BX), d.g.ly);
+    LBGPU_DISPATCH(d, (k_aa_even<S><<<grid, BX, 0, s>>>(d.g, B<S>(d, 0), d.tag, d.bc, d.omega,
+                       SIDE<S>(d, side_par), d.scale, d.inv_scale)));
+}
+
+void launch_aa_odd(const DevLattice &d, int side_par, cudaStream_t s)
+{
+    dim3 grid(cdiv(d.g.lx, BX), d.g.ly);
+    LBGPU_DISPATCH(d, (k_aa_odd<S><<<grid, BX, 0, s>>>(d.g, B<S>(d, 0), d.tag, d.bc, d.omega,
+                       SIDE<S>(d, side_par), d.scale, d.inv_scale)));
+}
+
+void launch_side_from_buf(const DevLattice &d, int b, int side_par, cudaStream_t s)
+{
+    const int n = 2 * d.g.lx + (d.g.ly > 2 ? 2 * (d.g.ly - 2) : 0);
+    LBGPU_DISPATCH(d, (k_side_from_buf<S><<<cdiv(n, 256), 256, 0, s>>>(d.g, B<S>(d, b),
+                       SIDE<S>(d, side_par))));
+}
+
+void launch_ghost_copy(const DevLattice &d, int b, cudaStream_t s)
+{
+    if (!d.ghost2) return;
+    LBGPU_DISPATCH(d, (k_ghost_copy<S><<<cdiv(d.g.nghost(), 256), 256, 0, s>>>(d.g, B<S>(d, b),
+                       static_cast<S *>(d.ghost2))));
+}
+
+void launch_readout(const DevLattice &d, int view, int cur, int side_par, int X0, int X1,
+                    double *out, int rec_stride, const uint64_t *dynp, cudaStream_t s)
+{
+    if (X1 <= X0) return;
+    dim3 grid(cdiv(d.g.ly + 2, BX), X1 - X0);
+    LBGPU_DISPATCH(d, (k_readout<S><<<grid, BX, 0, s>>>(d.g, view, B<S>(d, cur), OTHER<S>(d, cur),
+                       SIDE<S>(d, side_par), X0, X1, out, rec_stride, dynp, d.inv_scale)));
+}
+
+void launch_upload(const DevLattice &d, int b, const double *in, int rec_stride, int X0, int X1,
+                   cudaStream_t s)
+{
+    if (X1 <= X0) return;
+    dim3 grid(cdiv(d.g.ly + 2, BX), X1 - X0);
+    LBGPU_DISPATCH(d, (k_upload<S><<<grid, BX, 0, s>>>(d.g, in, rec_stride, X0, X1, B<S>(d, b),
+                       d.scale)));
+}
+
+void launch_zgb_rho(const DevLattice &d, int view, int cur, int side_par, cudaStream_t s)
+{
+    LBGPU_DISPATCH(d, (k_zgb_rho<S><<<cdiv(d.g.ly + 2, 128), 128, 0, s>>>(d.g, view, B<S>(d, cur),
+                       OTHER<S>(d, cur), SIDE<S>(d, side_par), d.zrho, d.inv_scale)));
+}
+
+void launch_zgb_apply(const DevLattice &d, cudaStream_t s)
+{
+    k_zgb_apply<<<cdiv(4LL * d.g.nb, 256), 256, 0, s>>>(d.g.nb, d.zgb_src, d.zrho, d.bc);
+}
+
+void launch_periodic(const DevLattice &d, int b, cudaStream_t s)
+{
+    LBGPU_DISPATCH(d, (k_periodic<S><<<1, 1024, 0, s>>>(d.g, B<S>(d, b))));
+}
+
+void launch_init_cylinder(const DevLattice &d, int b, double umax, cudaStream_t s)
+{
+    dim3 grid(cdiv(d.g.lx + 2, BX), d.g.ly + 2);
+    LBGPU_DISPATCH(d, (k_init_cylinder<S><<<grid, BX, 0, s>>>(d.g, B<S>(d, b), umax, d.scale)));
+}
+
+void launch_macros(const DevLattice &d, int view, int cur, int side_par, double *rho, double *ux,
+                   double *uy, cudaStream_t s)
+{
+    dim3 grid(cdiv(d.g.lx, BX), d.g.ly);
+    LBGPU_DISPATCH(d, (k_macros<S><<<grid, BX, 0, s>>>(d.g, view, B<S>(d, cur), OTHER<S>(d, cur),
+                       SIDE<S>(d, side_par), rho, ux, uy, d.inv_scale)));
+}
+
+}  // namespace lbgpu

@@ -9,8 +9,10 @@ namespace lbgpu {
 // Device-side view of one lattice's data, passed by value to the launchers.
 struct DevLattice {
     Geo g;
+    int precision;       // LBGPU_F64 / F32 / F16 / BF16: element type of buf and side
     void *buf[2];        // population buffers (buf[1] unused by the AA scheme)
     void *side;          // stale-slot store [2][9][nper]
+    void *ghost2;        // AA only: the second buffer's ghost ring [9][nghost] (see logical())
     const uint8_t *tag;  // tag plane
     double *bc;          // boundary tables [8][2][nb]
     const int *zgb_src;  // [4][nb]: pressure-table slot -> source row of its ZGB density, or -1
@@ -19,20 +21,32 @@ struct DevLattice {
     float scale, inv_scale;  // FP16/BF16 offset storage: stored = (f - w) * scale
 };
 
-// ---- exact FP64 kernels (reference arithmetic, bit-exact) ------------------------------
-void launch_collide_inplace_f64(const DevLattice &d, int cur, int side_par, cudaStream_t s);
-void launch_pull_f64(const DevLattice &d, int src, int side_par, bool ghosts, cudaStream_t s);
-void launch_stream_f64(const DevLattice &d, int src, int side_par, cudaStream_t s);
-void launch_side_from_buf_f64(const DevLattice &d, int b, int side_par, cudaStream_t s);
-void launch_readout_f64(const DevLattice &d, int cur, int pending, int side_par, int X0, int X1,
-                        double *out, int rec_stride, const uint64_t *dynp, cudaStream_t s);
-void launch_upload_f64(const DevLattice &d, int b, const double *in, int rec_stride, int X0,
-                       int X1, cudaStream_t s);
-void launch_zgb_rho_f64(const DevLattice &d, int cur, int pending, int side_par, cudaStream_t s);
+// How the post-stream state is read from a buffer:
+//   VIEW_DIRECT        the buffer holds it (pull form L, or a collided state read as is)
+//   VIEW_PULL_PENDING  the buffer holds C_n; the state is C_n streamed (side store: C_{n-1})
+//   VIEW_AA_NATURAL    AA buffer in natural slots; stale slots in the side store
+//   VIEW_AA_SWAPPED    AA buffer holds C_n in the opposite slots of each node
+enum { VIEW_DIRECT = 0, VIEW_PULL_PENDING = 1, VIEW_AA_NATURAL = 2, VIEW_AA_SWAPPED = 3 };
+
+void launch_collide_inplace(const DevLattice &d, int cur, int side_par, cudaStream_t s);
+void launch_pull(const DevLattice &d, int src, int side_par, bool ghosts, cudaStream_t s);
+void launch_stream(const DevLattice &d, int src, int side_par, cudaStream_t s);
+void launch_side_from_buf(const DevLattice &d, int b, int side_par, cudaStream_t s);
+// AA only: keep buffer b's ghost ring as the second buffer's (d.ghost2).
+void launch_ghost_copy(const DevLattice &d, int b, cudaStream_t s);
+void launch_readout(const DevLattice &d, int view, int cur, int side_par, int X0, int X1,
+                    double *out, int rec_stride, const uint64_t *dynp, cudaStream_t s);
+void launch_upload(const DevLattice &d, int b, const double *in, int rec_stride, int X0, int X1,
+                   cudaStream_t s);
+void launch_zgb_rho(const DevLattice &d, int view, int cur, int side_par, cudaStream_t s);
 void launch_zgb_apply(const DevLattice &d, cudaStream_t s);
-void launch_periodic_f64(const DevLattice &d, int b, cudaStream_t s);
-void launch_init_cylinder_f64(const DevLattice &d, int b, double umax, cudaStream_t s);
-void launch_macros_f64(const DevLattice &d, int cur, int pending, int side_par, double *rho,
-                       double *ux, double *uy, cudaStream_t s);
+void launch_periodic(const DevLattice &d, int b, cudaStream_t s);
+void launch_init_cylinder(const DevLattice &d, int b, double umax, cudaStream_t s);
+void launch_macros(const DevLattice &d, int view, int cur, int side_par, double *rho, double *ux,
+                   double *uy, cudaStream_t s);
+// AA scheme (buffer 0): the even step collides every node in place into the opposite slots,
+// the odd step gathers from the neighbours' opposite slots and scatters to their natural slots.
+void launch_aa_even(const DevLattice &d, int side_par, cudaStream_t s);
+void launch_aa_odd(const DevLattice &d, int side_par, cudaStream_t s);
 
 }  // namespace lbgpu

@@ -65,12 +65,10 @@ int Lattice::create(int lx_, int ly_, int precision_, int scheme_)
         return set_error(LB_ERR_ARG, "unknown precision %d", precision_);
     if (scheme_ != LBGPU_PULL && scheme_ != LBGPU_AA)
         return set_error(LB_ERR_ARG, "unknown scheme %d", scheme_);
-    if (precision_ != LBGPU_F64 || scheme_ != LBGPU_PULL)
-        return set_error(LB_ERR_ARG, "precision %d / scheme %d kernels are not built", precision_,
-                         scheme_);
     lx = lx_; ly = ly_; precision = precision_; scheme = scheme_;
     elem = elem_bytes(precision);
     d.g = make_geo(lx, ly, (int)elem);
+    d.precision = precision;
     d.omega = 1.0;
     d.scale = 1.0f; d.inv_scale = 1.0f;
     int ndev = 0;
@@ -88,6 +86,13 @@ int Lattice::create(int lx_, int ly_, int precision_, int scheme_)
         d.buf[b] = p;
         LB_CUDA(cudaMemsetAsync(p, 0, pbytes, stream), "cudaMemset(populations)");
     }
+    if (scheme == LBGPU_AA) {
+        const size_t gbytes = 9 * (size_t)d.g.nghost() * elem;
+        LB_CUDA(cudaMalloc(&p, gbytes), "cudaMalloc(ghost ring)");
+        d.ghost2 = p;
+        LB_CUDA(cudaMemsetAsync(p, 0, gbytes, stream), "cudaMemset(ghost ring)");
+        bytes += gbytes;
+    }
     LB_CUDA(cudaMalloc(&p, sbytes), "cudaMalloc(side store)");
     d.side = p;
     LB_CUDA(cudaMemsetAsync(p, 0, sbytes, stream), "cudaMemset(side store)");
@@ -103,7 +108,7 @@ int Lattice::create(int lx_, int ly_, int precision_, int scheme_)
     LB_CUDA(cudaMalloc(&p, 2 * (size_t)(ly + 2) * sizeof(double)), "cudaMalloc(zgb rho)");
     d.zrho = static_cast<double *>(p);
     LB_CUDA(cudaMemsetAsync(p, 0, 2 * (size_t)(ly + 2) * sizeof(double), stream), "cudaMemset");
-    bytes = nbuf * pbytes + sbytes + (size_t)d.g.plane + 16 * (size_t)d.g.nb * 8 +
+    bytes += nbuf * pbytes + sbytes + (size_t)d.g.plane + 16 * (size_t)d.g.nb * 8 +
             4 * (size_t)d.g.nb * 4 + 2 * (size_t)(ly + 2) * 8;
     bc_host.assign(16 * (size_t)d.g.nb, 0.0);
     zgb_src_host.assign(4 * (size_t)d.g.nb, -1);
@@ -116,6 +121,7 @@ void Lattice::destroy()
     if (stream) cudaStreamSynchronize(stream);
     for (int b = 0; b < 2; ++b) if (d.buf[b]) cudaFree(d.buf[b]);
     if (d.side) cudaFree(d.side);
+    if (d.ghost2) cudaFree(d.ghost2);
     if (d.tag) cudaFree(const_cast<uint8_t *>(d.tag));
     if (d.bc) cudaFree(d.bc);
     if (d.zgb_src) cudaFree(const_cast<int *>(d.zgb_src));
@@ -131,15 +137,28 @@ int Lattice::check(const char *what)
     return cuda_error(cudaGetLastError(), what);
 }
 
-// ---- state machine --------------------------------------------------------------------
+// How the post-stream state is read, and which side parity holds its stale slots.
+void Lattice::view(int &v, int &par) const
+{
+    if (scheme == LBGPU_AA) {
+        if (form == FORM_L) { v = VIEW_AA_NATURAL; par = (int)(n & 1); }
+        else { v = VIEW_AA_SWAPPED; par = (int)((n + 1) & 1); }
+        return;
+    }
+    par = (int)((n + 1) & 1);
+    v = (form == FORM_C && pending) ? VIEW_PULL_PENDING : VIEW_DIRECT;
+}
+
+// ---- state machine (pull scheme) ------------------------------------------------------
 int Lattice::op_collide()
 {
+    if (scheme != LBGPU_PULL) return set_error(LB_ERR_STATE, "collide/propagate need the pull scheme");
     if (form == FORM_C && pending) {
-        launch_pull_f64(d, cur, (int)((n + 1) & 1), ghosts, stream);
+        launch_pull(d, cur, (int)((n + 1) & 1), ghosts, stream);
         cur = 1 - cur;
         ++n;
     } else {
-        launch_collide_inplace_f64(d, cur, (int)(n & 1), stream);
+        launch_collide_inplace(d, cur, (int)(n & 1), stream);
         form = FORM_C;
     }
     pending = 0;
@@ -149,8 +168,9 @@ int Lattice::op_collide()
 
 int Lattice::materialize()
 {
+    if (scheme != LBGPU_PULL) return set_error(LB_ERR_STATE, "materialize needs the pull scheme");
     if (form == FORM_C && pending) {
-        launch_stream_f64(d, cur, (int)((n + 1) & 1), stream);
+        launch_stream(d, cur, (int)((n + 1) & 1), stream);
         cur = 1 - cur;
         ++n;
         form = FORM_L;
@@ -162,13 +182,14 @@ int Lattice::materialize()
 
 int Lattice::op_propagate()
 {
+    if (scheme != LBGPU_PULL) return set_error(LB_ERR_STATE, "collide/propagate need the pull scheme");
     if (form == FORM_C && !pending) {
         pending = 1;
         return LB_OK;
     }
     LB_TRY(materialize());
     // stream of an uncollided state: it acts as its own post-collision state
-    launch_side_from_buf_f64(d, cur, (int)(n & 1), stream);
+    launch_side_from_buf(d, cur, (int)(n & 1), stream);
     ++launches;
     form = FORM_C;
     pending = 1;
@@ -178,12 +199,32 @@ int Lattice::op_propagate()
 int Lattice::zgb_pass()
 {
     if (lx < 2) return set_error(LB_ERR_ARG, "the extrapolated outlet needs lx >= 2");
-    if (form == FORM_C && !pending)
+    if (scheme == LBGPU_PULL && form == FORM_C && !pending)
         return set_error(LB_ERR_STATE, "extrapolated outlet requested on a collided state");
-    launch_zgb_rho_f64(d, cur, form == FORM_C ? 1 : 0, (int)((n + 1) & 1), stream);
+    int v, par;
+    view(v, par);
+    launch_zgb_rho(d, v, cur, par, stream);
     launch_zgb_apply(d, stream);
     launches += 2;
     return check("zgb pass");
+}
+
+// One AA time step: natural form -> even kernel (C_m into the opposite slots); swapped form ->
+// odd kernel (gather, collide, scatter), leaving the natural form two steps on.
+int Lattice::aa_step()
+{
+    if (form == FORM_L) {
+        launch_aa_even(d, (int)(n & 1), stream);
+        form = FORM_C;
+        pending = 1;
+    } else {
+        launch_aa_odd(d, (int)((n + 1) & 1), stream);
+        n += 2;
+        form = FORM_L;
+        pending = 0;
+    }
+    ++launches;
+    return check("aa step");
 }
 
 int Lattice::step(int nsteps)
@@ -192,10 +233,20 @@ int Lattice::step(int nsteps)
     launches = 0;
     for (int s = 0; s < nsteps; ++s) {
         if (zgb_each_step) LB_TRY(zgb_pass());
-        LB_TRY(op_collide());
-        LB_TRY(op_propagate());
+        if (scheme == LBGPU_AA) {
+            LB_TRY(aa_step());
+        } else {
+            LB_TRY(op_collide());
+            LB_TRY(op_propagate());
+        }
     }
     return LB_OK;
+}
+
+long long Lattice::steps_done() const
+{
+    if (form == FORM_C && pending) return n + 1;
+    return n;
 }
 
 // ---- data movement --------------------------------------------------------------------
@@ -229,7 +280,7 @@ int Lattice::upload_records(int b, const double *host, int rs, int X0, int X1)
         LB_CUDA(cudaMemcpyAsync(stage, host + (size_t)(c0 - X0) * col,
                                 (size_t)(c1 - c0) * col * sizeof(double),
                                 cudaMemcpyHostToDevice, stream), "upload populations");
-        launch_upload_f64(d, b, stage, rs, c0, c1, stream);
+        launch_upload(d, b, stage, rs, c0, c1, stream);
         ++launches;
     }
     return check("upload");
@@ -240,10 +291,11 @@ int Lattice::readout_records(double *host, int rs, const uint64_t *dynp_dev, int
     const size_t col = (size_t)(ly + 2) * rs;
     const size_t cols = stage_cols(rs);
     LB_TRY(ensure_stage(cols * col * sizeof(double)));
-    const int pend = (form == FORM_C && pending) ? 1 : 0;
+    int v, par;
+    view(v, par);
     for (int c0 = X0; c0 < X1; c0 += (int)cols) {
         const int c1 = (c0 + (int)cols < X1) ? c0 + (int)cols : X1;
-        launch_readout_f64(d, cur, pend, (int)((n + 1) & 1), c0, c1, stage, rs, dynp_dev, stream);
+        launch_readout(d, v, cur, par, c0, c1, stage, rs, dynp_dev, stream);
         ++launches;
         LB_CUDA(cudaMemcpyAsync(host + (size_t)(c0 - X0) * col, stage,
                                 (size_t)(c1 - c0) * col * sizeof(double),
@@ -255,14 +307,14 @@ int Lattice::readout_records(double *host, int rs, const uint64_t *dynp_dev, int
 
 int Lattice::init_side_from(int b, int par)
 {
-    launch_side_from_buf_f64(d, b, par, stream);
+    launch_side_from_buf(d, b, par, stream);
     ++launches;
     return check("side store init");
 }
 
 int Lattice::init_cylinder(double umax)
 {
-    launch_init_cylinder_f64(d, 0, umax, stream);
+    launch_init_cylinder(d, 0, umax, stream);
     ++launches;
     return check("init cylinder");
 }
@@ -272,8 +324,9 @@ int Lattice::get_macros(double *rho, double *ux, double *uy)
     const size_t nn = (size_t)lx * ly;
     double *dev = nullptr;
     LB_CUDA(cudaMalloc(&dev, 3 * nn * sizeof(double)), "cudaMalloc(macros)");
-    const int pend = (form == FORM_C && pending) ? 1 : 0;
-    launch_macros_f64(d, cur, pend, (int)((n + 1) & 1), dev, dev + nn, dev + 2 * nn, stream);
+    int v, par;
+    view(v, par);
+    launch_macros(d, v, cur, par, dev, dev + nn, dev + 2 * nn, stream);
     int rc = check("macros");
     if (rc == LB_OK && rho) rc = cuda_error(cudaMemcpyAsync(rho, dev, nn * 8, cudaMemcpyDeviceToHost, stream), "macros");
     if (rc == LB_OK && ux) rc = cuda_error(cudaMemcpyAsync(ux, dev + nn, nn * 8, cudaMemcpyDeviceToHost, stream), "macros");

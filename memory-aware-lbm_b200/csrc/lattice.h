@@ -24,7 +24,7 @@ struct Lattice {
     DevLattice d{};
     size_t elem = 8;     // bytes per stored population
     int cur = 0;         // buffer holding the state
-    int form = FORM_L;   // see kernels_f64.cu
+    int form = FORM_L;   // see kernels.cu
     int pending = 0;     // form C only: 1 when the post-stream state is the current one
     long long n = 0;     // index of the last collision (form C) or of the state (form L)
     bool ghosts = false; // keep the ghost ring exact (drop-in interface)
@@ -47,7 +47,10 @@ struct Lattice {
     int op_propagate();      // mark (or perform) the stream
     int materialize();       // form C + pending -> form L
     int zgb_pass();          // extrapolated outlet densities into the tables (zgb_src slots)
+    int aa_step();           // one AA time step (even or odd kernel)
     int step(int nsteps);    // full native steps
+    void view(int &v, int &par) const;  // read-out view and stale side parity of the state
+    long long steps_done() const;
 
     // data movement
     int upload_bc(const double *bc);      // host [16*nb]

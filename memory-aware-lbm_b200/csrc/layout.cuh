@@ -45,6 +45,16 @@ struct Geo {
         if (X == 1) return 2 * lx + Y - 2;
         return 2 * lx + ly + Y - 2;
     }
+    // Ghost-ring numbering: row Y=0, row Y=ly+1 (X = 0..lx+1), then columns X=0 and
+    // X=lx+1 for Y = 1..ly; nghost() entries.
+    __host__ __device__ __forceinline__ int nghost() const { return 2 * (lx + 2) + 2 * ly; }
+    __host__ __device__ __forceinline__ int gidx(int X, int Y) const
+    {
+        if (Y == 0) return X;
+        if (Y == ly + 1) return lx + 2 + X;
+        if (X == 0) return 2 * (lx + 2) + Y - 1;
+        return 2 * (lx + 2) + ly + Y - 1;
+    }
 };
 
 // Build the geometry of an lx x ly lattice whose elements are `elem_bytes` wide.

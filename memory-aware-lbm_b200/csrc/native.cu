@@ -114,16 +114,36 @@ int lbgpu_set_populations(lbgpu_lattice *h, const double *f, const double *tmp)
     if (!f) return set_error(LB_ERR_ARG, "lbgpu_set_populations: null populations");
     Lattice &L = h->L;
     L.launches = 0;
-    if (int rc = L.upload_records(0, f, 9, 0, L.lx + 2)) return rc;
-    if (tmp) {
-        if (int rc = L.upload_records(1, tmp, 9, 0, L.lx + 2)) return rc;
+    if (L.scheme == LBGPU_AA) {
+        // one buffer: the second buffer only matters through its stale slots (side parity 1,
+        // read by the first odd step); the first buffer's own stale slots go to parity 0
+        // and, for odd step counts, through the ghost slots nothing streams into (ghost2)
+        if (tmp) {
+            if (int rc = L.upload_records(0, tmp, 9, 0, L.lx + 2)) return rc;
+            if (int rc = L.init_side_from(0, 1)) return rc;
+            lbgpu::launch_ghost_copy(L.d, 0, L.stream);
+        } else {
+            if (int rc = lbgpu::cuda_error(cudaMemsetAsync(L.d.side, 0, 2 * 9 * (size_t)L.d.g.nper * L.elem,
+                                                           L.stream), "clear side store"))
+                return rc;
+            if (int rc = lbgpu::cuda_error(cudaMemsetAsync(L.d.ghost2, 0, 9 * (size_t)L.d.g.nghost() * L.elem,
+                                                           L.stream), "clear ghost ring"))
+                return rc;
+        }
+        if (int rc = L.upload_records(0, f, 9, 0, L.lx + 2)) return rc;
+        if (int rc = L.init_side_from(0, 0)) return rc;
     } else {
-        if (int rc = lbgpu::cuda_error(cudaMemsetAsync(L.d.buf[1], 0, 9 * (size_t)L.d.g.plane * L.elem,
-                                                       L.stream), "clear second buffer"))
-            return rc;
+        if (int rc = L.upload_records(0, f, 9, 0, L.lx + 2)) return rc;
+        if (tmp) {
+            if (int rc = L.upload_records(1, tmp, 9, 0, L.lx + 2)) return rc;
+        } else {
+            if (int rc = lbgpu::cuda_error(cudaMemsetAsync(L.d.buf[1], 0, 9 * (size_t)L.d.g.plane * L.elem,
+                                                           L.stream), "clear second buffer"))
+                return rc;
+        }
+        // the first stream leaves the second buffer's content in the stale slots: side parity 1
+        if (int rc = L.init_side_from(1, 1)) return rc;
     }
-    // the first stream leaves the second buffer's content in the stale slots: side parity 1
-    if (int rc = L.init_side_from(1, 1)) return rc;
     L.cur = 0; L.form = lbgpu::FORM_L; L.pending = 0; L.n = 0;
     return lbgpu::cuda_error(cudaStreamSynchronize(L.stream), "lbgpu_set_populations");
 }
@@ -147,8 +167,18 @@ int lbgpu_setup_cylinder(lbgpu_lattice *h, int obst_x, int obst_y, int obst_r, d
             if (int rc = lbgpu::cuda_error(cudaMemsetAsync(L.d.buf[b], 0, 9 * (size_t)L.d.g.plane * L.elem,
                                                            L.stream), "clear populations"))
                 return rc;
+    if (int rc = lbgpu::cuda_error(cudaMemsetAsync(L.d.side, 0, 2 * 9 * (size_t)L.d.g.nper * L.elem,
+                                                   L.stream), "clear side store"))
+        return rc;
     if (int rc = L.init_cylinder(umax)) return rc;
-    if (int rc = L.init_side_from(1, 1)) return rc;
+    // second buffer zero (reference calloc, lb.c:91-92): side parity 1 stays zero; the AA scheme
+    // reads the initial state's own stale slots from parity 0
+    if (L.scheme == LBGPU_AA) {
+        if (int rc = L.init_side_from(0, 0)) return rc;
+        if (int rc = lbgpu::cuda_error(cudaMemsetAsync(L.d.ghost2, 0, 9 * (size_t)L.d.g.nghost() * L.elem,
+                                                       L.stream), "clear ghost ring"))
+            return rc;
+    }
     L.cur = 0; L.form = lbgpu::FORM_L; L.pending = 0; L.n = 0;
     return lbgpu::cuda_error(cudaStreamSynchronize(L.stream), "lbgpu_setup_cylinder");
 }
@@ -203,8 +233,7 @@ int lbgpu_synchronize(lbgpu_lattice *h)
 void *lbgpu_stream(lbgpu_lattice *h) { return h ? (void *)h->L.stream : nullptr; }
 long long lbgpu_steps_done(lbgpu_lattice *h)
 {
-    if (!h) return 0;
-    return h->L.n + ((h->L.form == lbgpu::FORM_C && h->L.pending) ? 1 : 0);
+    return h ? h->L.steps_done() : 0;
 }
 size_t lbgpu_device_bytes(lbgpu_lattice *h) { return h ? h->L.bytes : 0; }
 int lbgpu_last_kernel_launches(lbgpu_lattice *h) { return h ? h->L.launches : 0; }

@@ -73,9 +73,9 @@ extern "C" int lbgpu_get_macros_noalloc(lbgpu_lattice *h, double *rho, double *u
     double *s = nullptr;
     int rc = scratch_address(L.device, &s);
     if (rc == LB_OK) {
-        const int pend = (L.form == lbgpu::FORM_C && L.pending) ? 1 : 0;
-        lbgpu::launch_macros_f64(L.d, L.cur, pend, (int)((L.n + 1) & 1), s, s + nodes,
-                                 s + 2 * nodes, L.stream);
+        int v, par;
+        L.view(v, par);
+        lbgpu::launch_macros(L.d, v, L.cur, par, s, s + nodes, s + 2 * nodes, L.stream);
         rc = L.check("lbgpu_get_macros_noalloc");
     }
     double *dst[3] = {rho, ux, uy};
