@@ -153,6 +153,21 @@ int lbgpu_get_macros(lbgpu_lattice *lat, double *rho, double *ux, double *uy);
  * on the GPU race. */
 int lbgpu_get_macros_noalloc(lbgpu_lattice *lat, double *rho, double *ux, double *uy);
 
+/* FP64 sums over the current state, computed on the device in a fixed order (bitwise
+ * reproducible): out[0] mass (sum of rho over interior nodes), out[1..2] momentum, out[3..4]
+ * force on the obstacle by momentum exchange (2 c_i f_i over every link entering a bounce-back
+ * node strictly inside the lattice from a non-bounce-back node), out[5] kinetic energy of bulk
+ * nodes, out[6] number of nodes with a non-finite population, out[7] mass of bulk nodes.
+ * No counterpart in the reference (it computes no forces). */
+int lbgpu_moments(lbgpu_lattice *lat, double out[8]);
+
+/* Time averages of the velocity field: accumulate adds the current (ux, uy) of every interior
+ * node to FP64 running sums on the device; average copies sum/samples into [ly][lx] host arrays;
+ * reset clears the sums. */
+int lbgpu_velocity_accumulate(lbgpu_lattice *lat);
+int lbgpu_velocity_average(lbgpu_lattice *lat, double *ux, double *uy, long long *samples);
+int lbgpu_velocity_reset(lbgpu_lattice *lat);
+
 int lbgpu_synchronize(lbgpu_lattice *lat);
 void *lbgpu_stream(lbgpu_lattice *lat);           /* the lattice's cudaStream_t            */
 long long lbgpu_steps_done(lbgpu_lattice *lat);

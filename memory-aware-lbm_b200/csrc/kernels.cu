@@ -89,6 +89,118 @@ __device__ __forceinline__ typename Codec<S>::R logical(const Geo &g, int view, 
     }
 }
 
+// ---- 16-bit storage, four nodes per thread ------------------------------------------------
+//
+// Stored value D_i = (f_i - w_i) 2^s.  With sum(w) = 1 and sum(c w) = 0 the BGK step works on
+// D directly: rho = 1 + 2^-s sum(D), j = 2^-s sum(c D), and
+//   D_i' = D_i + omega (E_i - D_i),  E_i = 2^s w_i (rho (1 + 3 cu + 4.5 cu^2 - 1.5 u^2) - 1),
+// so there is no per-population decode or encode arithmetic, only the conversions (two per
+// instruction when packing).  Boundary rules decode to f and use the generic path.
+
+template <class S> struct Half2Ops;
+template <> struct Half2Ops<__half> {
+    static __device__ __forceinline__ float lo(unsigned w) { return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu))); }
+    static __device__ __forceinline__ float hi(unsigned w) { return __half2float(__ushort_as_half((unsigned short)(w >> 16))); }
+    static __device__ __forceinline__ unsigned pack(float a, float b)
+    {
+        const __half2 h = __floats2half2_rn(a, b);
+        return *reinterpret_cast<const unsigned *>(&h);
+    }
+};
+template <> struct Half2Ops<__nv_bfloat16> {
+    static __device__ __forceinline__ float lo(unsigned w) { return __uint_as_float(w << 16); }
+    static __device__ __forceinline__ float hi(unsigned w) { return __uint_as_float(w & 0xffff0000u); }
+    static __device__ __forceinline__ unsigned pack(float a, float b)
+    {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        return *reinterpret_cast<const unsigned *>(&h);
+    }
+};
+
+// BGK on scaled offsets D[9] of one node.  Opposite directions i, opp(i) share cu (up to sign):
+// E_i, E_opp = a +- b with a = 2^s w (A + 4.5 rho cu^2), b = 2^s w 3 rho cu, A = rho(1-1.5u^2)-1.
+// 1/rho uses the hardware reciprocal (the 16-bit path is held to a tolerance, not bit-exact).
+__device__ __forceinline__ void bgk_offsets(float D[9], float omega, float sc, float inv)
+{
+    const float sum = ((D[0] + D[1]) + (D[2] + D[3])) + ((D[4] + D[5]) + (D[6] + D[7])) + D[8];
+    const float rho = fmaf(inv, sum, 1.0f);
+    const float jx = inv * ((D[1] - D[3]) + (D[5] - D[6]) + (D[8] - D[7]));
+    const float jy = inv * ((D[2] - D[4]) + (D[5] - D[8]) + (D[6] - D[7]));
+    const float ir = __fdividef(1.0f, rho);
+    const float ux = jx * ir, uy = jy * ir;
+    const float A = fmaf(rho, fmaf(-1.5f, fmaf(ux, ux, uy * uy), 1.0f), -1.0f);
+    const float w1 = sc * (1.f / 9.f), w2 = sc * (1.f / 36.f);
+    D[0] = fmaf(omega, (sc * (4.f / 9.f)) * A - D[0], D[0]);
+#define LBGPU_PAIR(I, J, W, CU)                                        \
+    {                                                                  \
+        const float cu = (CU);                                         \
+        const float rcu = rho * cu;                                    \
+        const float a = W * fmaf(4.5f * cu, rcu, A);                   \
+        const float b = (3.0f * W) * rcu;                              \
+        D[I] = fmaf(omega, (a + b) - D[I], D[I]);                      \
+        D[J] = fmaf(omega, (a - b) - D[J], D[J]);                      \
+    }
+    LBGPU_PAIR(1, 3, w1, ux)
+    LBGPU_PAIR(2, 4, w1, uy)
+    LBGPU_PAIR(5, 7, w2, ux + uy)
+    LBGPU_PAIR(6, 8, w2, uy - ux)
+#undef LBGPU_PAIR
+}
+
+// Working values of a kernel: decoded populations f for FP64/FP32, the stored offsets D as
+// float for 16-bit storage (see bgk_offsets); collide_w applies a node's rule to them.  Every
+// kernel of one storage type uses these, so all schemes agree bit for bit.
+template <class S> struct Work {
+    using W = typename Codec<S>::R;
+    static __device__ __forceinline__ W load(S v, int i, float inv) { return Codec<S>::dec(v, i, inv); }
+    static __device__ __forceinline__ S store(W w, int i, float sc) { return Codec<S>::enc(w, i, sc); }
+};
+template <> struct Work<__half> {
+    using W = float;
+    static __device__ __forceinline__ float load(__half v, int, float) { return __half2float(v); }
+    static __device__ __forceinline__ __half store(float w, int, float) { return __float2half_rn(w); }
+};
+template <> struct Work<__nv_bfloat16> {
+    using W = float;
+    static __device__ __forceinline__ float load(__nv_bfloat16 v, int, float) { return __bfloat162float(v); }
+    static __device__ __forceinline__ __nv_bfloat16 store(float w, int, float) { return __float2bfloat16_rn(w); }
+};
+
+// A non-BGK rule on one node's 16-bit offsets: decode, the generic rule, encode.  Out of line so
+// the bulk path keeps its registers (it runs for boundary and obstacle nodes only).
+template <class S>
+static __device__ __noinline__ void boundary_offsets(const double *__restrict__ bc, Geo g, int t, int X,
+                                                     int Y, float D[9], double omega, float sc, float inv)
+{
+    float f[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) f[i] = fmaf(D[i], inv, wgtf(i));
+    collide_node<S>(bc, g, t, X, Y, f, omega);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) D[i] = (f[i] - wgtf(i)) * sc;
+}
+
+template <class S>
+__device__ __forceinline__ void collide_w(const double *__restrict__ bc, const Geo &g, int t, int X,
+                                          int Y, typename Work<S>::W w[9], double omega, float sc,
+                                          float inv)
+{
+    if constexpr (sizeof(S) == 2) {
+        if (t == TAG_BGK) {
+            bgk_offsets(w, (float)omega, sc, inv);
+        } else {
+            float tmp[9];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) tmp[i] = w[i];
+            boundary_offsets<S>(bc, g, t, X, Y, tmp, omega, sc, inv);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) w[i] = tmp[i];
+        }
+    } else {
+        collide_node<S>(bc, g, t, X, Y, w, omega);
+    }
+}
+
 // ---- pull scheme --------------------------------------------------------------------------
 
 // In-place collision of every interior node (form L -> form C); the perimeter nodes also
@@ -105,17 +217,17 @@ __global__ void __launch_bounds__(BX) k_collide_inplace(Geo g, S *__restrict__ b
     const int Y = blockIdx.y + 1;
     if (X > g.lx) return;
     const long long o = g.idx(X, Y);
-    R f[9];
+    typename Work<S>::W f[9];
 #pragma unroll
-    for (int i = 0; i < 9; ++i) f[i] = C::dec(plane(buf, g, i)[o], i, inv);
-    collide_node<S>(bc, g, tag[o], X, Y, f, omega);
+    for (int i = 0; i < 9; ++i) f[i] = Work<S>::load(plane(buf, g, i)[o], i, inv);
+    collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) plane(buf, g, i)[o] = C::enc(f[i], i, sc);
+    for (int i = 0; i < 9; ++i) plane(buf, g, i)[o] = Work<S>::store(f[i], i, sc);
     if (g.perimeter(X, Y)) {
         const int p = g.pidx(X, Y);
 #pragma unroll
         for (int i = 0; i < 9; ++i)
-            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = C::enc(f[i], i, sc);
+            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
     }
 }
 
@@ -144,29 +256,127 @@ __global__ void __launch_bounds__(BX) k_pull(Geo g, const S *__restrict__ src, S
         }
         return;
     }
-    R f[9];
+    typename Work<S>::W f[9];
     const bool edge = g.perimeter(X, Y);
     if (!edge) {
 #pragma unroll
         for (int i = 0; i < 9; ++i)
-            f[i] = C::dec(plane(src, g, i)[o - cx(i) - (long long)cy(i) * g.pitch], i, inv);
+            f[i] = Work<S>::load(plane(src, g, i)[o - cx(i) - (long long)cy(i) * g.pitch], i, inv);
     } else {
         const int p = g.pidx(X, Y);
 #pragma unroll
         for (int i = 0; i < 9; ++i) {
             const int sx = X - cx(i), sy = Y - cy(i);
-            f[i] = C::dec(g.interior(sx, sy) ? plane(src, g, i)[g.idx(sx, sy)]
+            f[i] = Work<S>::load(g.interior(sx, sy) ? plane(src, g, i)[g.idx(sx, sy)]
                                              : side[(size_t)i * g.nper + p], i, inv);
         }
     }
-    collide_node<S>(bc, g, tag[o], X, Y, f, omega);
+    collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = C::enc(f[i], i, sc);
+    for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = Work<S>::store(f[i], i, sc);
     if (edge) {
         const int p = g.pidx(X, Y);
 #pragma unroll
         for (int i = 0; i < 9; ++i)
-            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = C::enc(f[i], i, sc);
+            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
+    }
+}
+
+// Pull step for 16-bit storage, four nodes per thread (X = x0..x0+3, x0 = 1 + 4t, so a quad is
+// one aligned 8-byte word pair).  Interior warps: per direction one aligned 8-byte load, the
+// x-shifted quad assembled from the adjacent lane's word (one 32-bit shuffle) and byte
+// permutes; edge lanes take the neighbouring word from a second load whose address differs only
+// in that lane.  Warps touching the perimeter or the row's end run the per-node path.  The
+// kernel is bounded by instruction issue, so the collision is written for few instructions
+// (bgk_offsets) and the boundary rules stay out of line.
+template <class S>
+__device__ __forceinline__ void pull_node(const Geo &g, const S *__restrict__ src, S *__restrict__ dst,
+                                          const uint8_t *__restrict__ tag, const double *__restrict__ bc,
+                                          double omega, S *__restrict__ side, float sc, float inv,
+                                          int X, int Y)
+{
+    const long long o = g.idx(X, Y);
+    typename Work<S>::W f[9];
+    const bool edge = g.perimeter(X, Y);
+    const int p = edge ? g.pidx(X, Y) : 0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const int sx = X - cx(i), sy = Y - cy(i);
+        f[i] = Work<S>::load(g.interior(sx, sy) ? plane(src, g, i)[g.idx(sx, sy)]
+                                                : side[(size_t)i * g.nper + p], i, inv);
+    }
+    collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = Work<S>::store(f[i], i, sc);
+    if (edge) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
+    }
+}
+
+template <class S>
+__global__ void __launch_bounds__(BX) k_pull4h(Geo g, const S *__restrict__ src, S *__restrict__ dst,
+                                               const uint8_t *__restrict__ tag,
+                                               const double *__restrict__ bc, double omega,
+                                               S *__restrict__ side, float sc, float inv)
+{
+    using H = Half2Ops<S>;
+    const int t = blockIdx.x * BX + threadIdx.x;
+    const int x0 = 1 + 4 * t;
+    const int Y = blockIdx.y + 1;
+    const int lane = threadIdx.x & 31;
+    const int xw0 = x0 - 4 * lane;
+    const bool vec = (xw0 >= 2) && (xw0 + 127 <= g.lx - 1) && (Y >= 2) && (Y <= g.ly - 1);
+    if (!vec) {
+        for (int k = 0; k < 4; ++k)
+            if (x0 + k <= g.lx) pull_node<S>(g, src, dst, tag, bc, omega, side, sc, inv, x0 + k, Y);
+        return;
+    }
+    const long long o = g.idx(x0, Y);
+    uint2 v[9];
+    unsigned e[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const S *row = plane(src, g, i) + (o - (long long)cy(i) * g.pitch);
+        v[i] = *reinterpret_cast<const uint2 *>(row);
+        if (cx(i) == 1) e[i] = *reinterpret_cast<const unsigned *>(lane == 0 ? row - 2 : row);
+        if (cx(i) == -1) e[i] = *reinterpret_cast<const unsigned *>(lane == 31 ? row + 4 : row);
+    }
+    const unsigned tq = *reinterpret_cast<const unsigned *>(tag + o);
+    float D[4][9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        unsigned w0 = v[i].x, w1 = v[i].y;
+        if (cx(i) == 1) {            // quad of sources x0-1..x0+2
+            unsigned pw = __shfl_up_sync(0xffffffffu, v[i].y, 1);
+            if (lane == 0) pw = e[i];
+            const unsigned n0 = __byte_perm(pw, w0, 0x5432), n1 = __byte_perm(w0, w1, 0x5432);
+            w0 = n0; w1 = n1;
+        } else if (cx(i) == -1) {    // quad of sources x0+1..x0+4
+            unsigned nw = __shfl_down_sync(0xffffffffu, v[i].x, 1);
+            if (lane == 31) nw = e[i];
+            const unsigned n0 = __byte_perm(w0, w1, 0x5432), n1 = __byte_perm(w1, nw, 0x5432);
+            w0 = n0; w1 = n1;
+        }
+        D[0][i] = H::lo(w0); D[1][i] = H::hi(w0);
+        D[2][i] = H::lo(w1); D[3][i] = H::hi(w1);
+    }
+    if (tq == 0x01010101u) {         // four bulk nodes
+        const float om = (float)omega;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) bgk_offsets(D[k], om, sc, inv);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            collide_w<S>(bc, g, (int)((tq >> (8 * k)) & 0xff), x0 + k, Y, D[k], omega, sc, inv);
+    }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        uint2 w;
+        w.x = H::pack(D[0][i], D[1][i]);
+        w.y = H::pack(D[2][i], D[3][i]);
+        *reinterpret_cast<uint2 *>(plane(dst, g, i) + o) = w;
     }
 }
 
@@ -207,19 +417,19 @@ __global__ void __launch_bounds__(BX) k_aa_even(Geo g, S *__restrict__ a,
     const long long o = g.idx(X, Y);
     const bool edge = g.perimeter(X, Y);
     const int p = edge ? g.pidx(X, Y) : 0;
-    R f[9];
+    typename Work<S>::W f[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
         const bool stale = edge && !g.interior(X - cx(i), Y - cy(i));
-        f[i] = C::dec(stale ? side[(size_t)i * g.nper + p] : plane(a, g, i)[o], i, inv);
+        f[i] = Work<S>::load(stale ? side[(size_t)i * g.nper + p] : plane(a, g, i)[o], i, inv);
     }
-    collide_node<S>(bc, g, tag[o], X, Y, f, omega);
+    collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) plane(a, g, opp(i))[o] = C::enc(f[i], i, sc);
+    for (int i = 0; i < 9; ++i) plane(a, g, opp(i))[o] = Work<S>::store(f[i], i, sc);
     if (edge) {
 #pragma unroll
         for (int i = 0; i < 9; ++i)
-            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = C::enc(f[i], i, sc);
+            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
     }
 }
 
@@ -242,27 +452,27 @@ __global__ void __launch_bounds__(BX) k_aa_odd(Geo g, S *__restrict__ a,
     const long long o = g.idx(X, Y);
     const bool edge = g.perimeter(X, Y);
     const int p = edge ? g.pidx(X, Y) : 0;
-    R f[9];
+    typename Work<S>::W f[9];
     if (!edge) {
 #pragma unroll
         for (int i = 0; i < 9; ++i)
-            f[i] = C::dec(plane(a, g, opp(i))[o - cx(i) - (long long)cy(i) * g.pitch], i, inv);
+            f[i] = Work<S>::load(plane(a, g, opp(i))[o - cx(i) - (long long)cy(i) * g.pitch], i, inv);
     } else {
 #pragma unroll
         for (int i = 0; i < 9; ++i) {
             const int sx = X - cx(i), sy = Y - cy(i);
-            f[i] = C::dec(g.interior(sx, sy) ? plane(a, g, opp(i))[g.idx(sx, sy)]
+            f[i] = Work<S>::load(g.interior(sx, sy) ? plane(a, g, opp(i))[g.idx(sx, sy)]
                                              : side[(size_t)i * g.nper + p], i, inv);
         }
     }
-    collide_node<S>(bc, g, tag[o], X, Y, f, omega);
+    collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
 #pragma unroll
     for (int i = 0; i < 9; ++i)
-        plane(a, g, i)[o + cx(i) + (long long)cy(i) * g.pitch] = C::enc(f[i], i, sc);
+        plane(a, g, i)[o + cx(i) + (long long)cy(i) * g.pitch] = Work<S>::store(f[i], i, sc);
     if (edge) {
 #pragma unroll
         for (int i = 0; i < 9; ++i)
-            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = C::enc(f[i], i, sc);
+            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
     }
 }
 
@@ -445,6 +655,114 @@ __global__ void __launch_bounds__(BX) k_macros(Geo g, int view, const S *__restr
     if (uy) uy[k] = (double)v;
 }
 
+// ---- FP64 reductions of the current state ----------------------------------------------
+//
+// One block per interior row sums, in a fixed order, eight quantities over the row into
+// partial[Y][8]; k_moments_final sums the rows in a fixed order.  Results are bitwise
+// reproducible for a given lattice and state.
+//   0 mass            sum of rho over every interior node
+//   1, 2 momentum     sum of (jx, jy)
+//   3, 4 force        momentum exchange on the obstacle: 2 sum c_i f_i over every link that
+//                     enters a bounce-back node strictly inside the lattice (rows 2..ly-1,
+//                     columns 2..lx-1) from a non-bounce-back node, f_i being the population
+//                     that arrived at the solid node this step (full-way bounce-back returns
+//                     it reversed: momentum 2 c_i f_i per link and step)
+//   5 kinetic energy  sum of |j|^2 / (2 rho) over bulk (BGK) nodes
+//   6 non-finite      number of nodes with a NaN or infinite population
+//   7 fluid mass      sum of rho over bulk (BGK) nodes
+constexpr int RED_THREADS = 256;
+
+template <class S>
+__global__ void __launch_bounds__(RED_THREADS) k_moments_rows(Geo g, int view, const S *__restrict__ cur,
+                                                              const S *__restrict__ other,
+                                                              const S *__restrict__ side,
+                                                              const uint8_t *__restrict__ tag,
+                                                              double *__restrict__ partial, float inv)
+{
+    const int Y = blockIdx.x + 1;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int X = 1 + threadIdx.x; X <= g.lx; X += RED_THREADS) {
+        double f[9];
+        bool bad = false;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            f[i] = (double)logical(g, view, cur, other, side, X, Y, i, inv);
+            bad |= !isfinite(f[i]);
+        }
+        const double rho = ((f[0] + f[1]) + (f[2] + f[3])) + ((f[4] + f[5]) + (f[6] + f[7])) + f[8];
+        const double jx = (f[1] - f[3]) + (f[5] - f[6]) + (f[8] - f[7]);
+        const double jy = (f[2] - f[4]) + (f[5] - f[8]) + (f[6] - f[7]);
+        acc[0] += rho; acc[1] += jx; acc[2] += jy;
+        acc[6] += bad ? 1.0 : 0.0;
+        const int t = tag[g.idx(X, Y)];
+        if (t == TAG_BGK) {
+            acc[5] += (jx * jx + jy * jy) / (2.0 * rho);
+            acc[7] += rho;
+        } else if (t == TAG_BOUNCE && X >= 2 && X <= g.lx - 1 && Y >= 2 && Y <= g.ly - 1) {
+#pragma unroll
+            for (int i = 1; i < 9; ++i) {
+                if (tag[g.idx(X - cx(i), Y - cy(i))] != TAG_BOUNCE) {
+                    acc[3] += 2.0 * cx(i) * f[i];
+                    acc[4] += 2.0 * cy(i) * f[i];
+                }
+            }
+        }
+    }
+    __shared__ double red[8][RED_THREADS];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) red[k][threadIdx.x] = acc[k];
+    __syncthreads();
+    for (int w = RED_THREADS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 8) partial[(size_t)Y * 8 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_moments_final(int ly, const double *__restrict__ partial,
+                                                               double *__restrict__ out)
+{
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int Y = 1 + threadIdx.x; Y <= ly; Y += RED_THREADS)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] += partial[(size_t)Y * 8 + k];
+    __shared__ double red[8][RED_THREADS];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) red[k][threadIdx.x] = acc[k];
+    __syncthreads();
+    for (int w = RED_THREADS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 8) out[threadIdx.x] = red[threadIdx.x][0];
+}
+
+// Running sums of the velocity field (time averages): acc[0][.] += ux, acc[1][.] += uy.
+template <class S>
+__global__ void __launch_bounds__(BX) k_accumulate_velocity(Geo g, int view, const S *__restrict__ cur,
+                                                            const S *__restrict__ other,
+                                                            const S *__restrict__ side,
+                                                            double *__restrict__ acc, float inv)
+{
+    const int X = blockIdx.x * BX + threadIdx.x + 1;
+    const int Y = blockIdx.y + 1;
+    if (X > g.lx) return;
+    double f[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) f[i] = (double)logical(g, view, cur, other, side, X, Y, i, inv);
+    const double rho = ((f[0] + f[1]) + (f[2] + f[3])) + ((f[4] + f[5]) + (f[6] + f[7])) + f[8];
+    const double jx = (f[1] - f[3]) + (f[5] - f[6]) + (f[8] - f[7]);
+    const double jy = (f[2] - f[4]) + (f[5] - f[8]) + (f[6] - f[7]);
+    const size_t k = (size_t)(Y - 1) * g.lx + (X - 1);
+    const size_t n = (size_t)g.lx * g.ly;
+    acc[k] += jx / rho;
+    acc[n + k] += jy / rho;
+}
+
 inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
 template <class S> S *B(const DevLattice &d, int b) { return static_cast<S *>(d.buf[b]); }
@@ -482,6 +800,17 @@ void launch_pull(const DevLattice &d, int src, int side_par, bool ghosts, cudaSt
         dim3 grid(cdiv(d.g.lx + 2, BX), d.g.ly + 2);
         LBGPU_DISPATCH(d, (k_pull<S, true><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src),
                            d.tag, d.bc, d.omega, SIDE<S>(d, side_par), d.scale, d.inv_scale)));
+    } else if (d.precision == LBGPU_F16 || d.precision == LBGPU_BF16) {
+        dim3 grid(cdiv((d.g.lx + 3) / 4, BX), d.g.ly);
+        if (d.precision == LBGPU_F16)
+            k_pull4h<__half><<<grid, BX, 0, s>>>(d.g, B<__half>(d, src), B<__half>(d, 1 - src), d.tag,
+                                                 d.bc, d.omega, SIDE<__half>(d, side_par), d.scale,
+                                                 d.inv_scale);
+        else
+            k_pull4h<__nv_bfloat16><<<grid, BX, 0, s>>>(d.g, B<__nv_bfloat16>(d, src),
+                                                        B<__nv_bfloat16>(d, 1 - src), d.tag, d.bc,
+                                                        d.omega, SIDE<__nv_bfloat16>(d, side_par),
+                                                        d.scale, d.inv_scale);
     } else {
         dim3 grid(cdiv(d.g.lx, BX), d.g.ly);
         LBGPU_DISPATCH(d, (k_pull<S, false><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src),
@@ -562,6 +891,22 @@ void launch_init_cylinder(const DevLattice &d, int b, double umax, cudaStream_t 
 {
     dim3 grid(cdiv(d.g.lx + 2, BX), d.g.ly + 2);
     LBGPU_DISPATCH(d, (k_init_cylinder<S><<<grid, BX, 0, s>>>(d.g, B<S>(d, b), umax, d.scale)));
+}
+
+void launch_moments(const DevLattice &d, int view, int cur, int side_par, double *partial,
+                    double *out, cudaStream_t s)
+{
+    LBGPU_DISPATCH(d, (k_moments_rows<S><<<d.g.ly, RED_THREADS, 0, s>>>(d.g, view, B<S>(d, cur),
+                       OTHER<S>(d, cur), SIDE<S>(d, side_par), d.tag, partial, d.inv_scale)));
+    k_moments_final<<<1, RED_THREADS, 0, s>>>(d.g.ly, partial, out);
+}
+
+void launch_accumulate_velocity(const DevLattice &d, int view, int cur, int side_par, double *acc,
+                                cudaStream_t s)
+{
+    dim3 grid(cdiv(d.g.lx, BX), d.g.ly);
+    LBGPU_DISPATCH(d, (k_accumulate_velocity<S><<<grid, BX, 0, s>>>(d.g, view, B<S>(d, cur),
+                       OTHER<S>(d, cur), SIDE<S>(d, side_par), acc, d.inv_scale)));
 }
 
 void launch_macros(const DevLattice &d, int view, int cur, int side_par, double *rho, double *ux,

@@ -44,6 +44,13 @@ void launch_periodic(const DevLattice &d, int b, cudaStream_t s);
 void launch_init_cylinder(const DevLattice &d, int b, double umax, cudaStream_t s);
 void launch_macros(const DevLattice &d, int view, int cur, int side_par, double *rho, double *ux,
                    double *uy, cudaStream_t s);
+// FP64 reductions of the current state (mass, momentum, obstacle force, kinetic energy,
+// non-finite nodes, fluid mass) into out[8]; `partial` is scratch of (ly+2)*8 doubles.
+void launch_moments(const DevLattice &d, int view, int cur, int side_par, double *partial,
+                    double *out, cudaStream_t s);
+// acc[0..lx*ly) += ux, acc[lx*ly..2*lx*ly) += uy of the current state.
+void launch_accumulate_velocity(const DevLattice &d, int view, int cur, int side_par, double *acc,
+                                cudaStream_t s);
 // AA scheme (buffer 0): the even step collides every node in place into the opposite slots,
 // the odd step gathers from the neighbours' opposite slots and scatters to their natural slots.
 void launch_aa_even(const DevLattice &d, int side_par, cudaStream_t s);

@@ -127,6 +127,9 @@ void Lattice::destroy()
     if (d.zgb_src) cudaFree(const_cast<int *>(d.zgb_src));
     if (d.zrho) cudaFree(d.zrho);
     if (stage) cudaFree(stage);
+    if (red_scratch) cudaFree(red_scratch);
+    if (vel_acc) cudaFree(vel_acc);
+    red_scratch = nullptr; vel_acc = nullptr; vel_samples = 0;
     if (stream) cudaStreamDestroy(stream);
     d = DevLattice{};
     stage = nullptr; stage_bytes = 0; stream = nullptr;
@@ -334,6 +337,56 @@ int Lattice::get_macros(double *rho, double *ux, double *uy)
     if (rc == LB_OK) rc = cuda_error(cudaStreamSynchronize(stream), "macros");
     cudaFree(dev);
     return rc;
+}
+
+int Lattice::moments(double out[8])
+{
+    if (!red_scratch) {
+        void *p = nullptr;
+        LB_CUDA(cudaMalloc(&p, ((size_t)(ly + 2) * 8 + 8) * sizeof(double)), "cudaMalloc(reduction)");
+        red_scratch = static_cast<double *>(p);
+    }
+    int v, par;
+    view(v, par);
+    double *res = red_scratch + (size_t)(ly + 2) * 8;
+    launch_moments(d, v, cur, par, red_scratch, res, stream);
+    LB_TRY(check("moments"));
+    LB_CUDA(cudaMemcpyAsync(out, res, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream), "moments");
+    LB_CUDA(cudaStreamSynchronize(stream), "moments");
+    return LB_OK;
+}
+
+int Lattice::velocity_accumulate()
+{
+    const size_t bytes = 2 * (size_t)lx * ly * sizeof(double);
+    if (!vel_acc) {
+        void *p = nullptr;
+        LB_CUDA(cudaMalloc(&p, bytes), "cudaMalloc(velocity sums)");
+        vel_acc = static_cast<double *>(p);
+        LB_CUDA(cudaMemsetAsync(vel_acc, 0, bytes, stream), "clear velocity sums");
+        vel_samples = 0;
+    }
+    int v, par;
+    view(v, par);
+    launch_accumulate_velocity(d, v, cur, par, vel_acc, stream);
+    ++vel_samples;
+    return check("velocity accumulate");
+}
+
+int Lattice::velocity_average(double *ux, double *uy, long long *samples)
+{
+    const size_t nn = (size_t)lx * ly;
+    if (samples) *samples = vel_samples;
+    if (!vel_acc || vel_samples == 0) return set_error(LB_ERR_STATE, "no velocity samples accumulated");
+    if (ux) LB_CUDA(cudaMemcpyAsync(ux, vel_acc, nn * 8, cudaMemcpyDeviceToHost, stream), "velocity average");
+    if (uy) LB_CUDA(cudaMemcpyAsync(uy, vel_acc + nn, nn * 8, cudaMemcpyDeviceToHost, stream), "velocity average");
+    LB_CUDA(cudaStreamSynchronize(stream), "velocity average");
+    const double k = 1.0 / (double)vel_samples;
+    for (size_t i = 0; i < nn; ++i) {
+        if (ux) ux[i] *= k;
+        if (uy) uy[i] *= k;
+    }
+    return LB_OK;
 }
 
 int Lattice::upload_bc(const double *bc)

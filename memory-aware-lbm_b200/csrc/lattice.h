@@ -62,6 +62,12 @@ struct Lattice {
     int init_side_from(int b, int par);
     int init_cylinder(double umax);  // equilibrium Poiseuille populations into buffer 0
     int get_macros(double *rho, double *ux, double *uy);  // host [ly][lx] arrays
+    int moments(double out[8]);                           // FP64 sums (kernels.h)
+    int velocity_accumulate();
+    int velocity_average(double *ux, double *uy, long long *samples);
+    double *red_scratch = nullptr;  // (ly+2)*8 partial sums + 8 results
+    double *vel_acc = nullptr;      // 2*lx*ly running velocity sums
+    long long vel_samples = 0;
     int check(const char *what);   // cudaGetLastError -> error code
     int side_par_stale() const { return (int)((n + 1) & 1); }
     size_t stage_cols(int rs) const;

@@ -224,6 +224,35 @@ int lbgpu_get_macros(lbgpu_lattice *h, double *rho, double *ux, double *uy)
     return h->L.get_macros(rho, ux, uy);
 }
 
+int lbgpu_moments(lbgpu_lattice *h, double out[8])
+{
+    if (int rc = bad_handle(h, "lbgpu_moments")) return rc;
+    if (!out) return set_error(LB_ERR_ARG, "lbgpu_moments: null output");
+    return h->L.moments(out);
+}
+
+int lbgpu_velocity_accumulate(lbgpu_lattice *h)
+{
+    if (int rc = bad_handle(h, "lbgpu_velocity_accumulate")) return rc;
+    return h->L.velocity_accumulate();
+}
+
+int lbgpu_velocity_average(lbgpu_lattice *h, double *ux, double *uy, long long *samples)
+{
+    if (int rc = bad_handle(h, "lbgpu_velocity_average")) return rc;
+    return h->L.velocity_average(ux, uy, samples);
+}
+
+int lbgpu_velocity_reset(lbgpu_lattice *h)
+{
+    if (int rc = bad_handle(h, "lbgpu_velocity_reset")) return rc;
+    lbgpu::Lattice &L = h->L;
+    L.vel_samples = 0;
+    if (!L.vel_acc) return LB_OK;
+    return lbgpu::cuda_error(cudaMemsetAsync(L.vel_acc, 0, 2 * (size_t)L.lx * L.ly * sizeof(double), L.stream),
+                             "lbgpu_velocity_reset");
+}
+
 int lbgpu_synchronize(lbgpu_lattice *h)
 {
     if (int rc = bad_handle(h, "lbgpu_synchronize")) return rc;

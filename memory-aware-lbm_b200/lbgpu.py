@@ -78,6 +78,10 @@ def lib():
     L.lbgpu_get_populations.argtypes = [_vp, _dp]
     L.lbgpu_get_macros.argtypes = [_vp, _dp, _dp, _dp]
     L.lbgpu_get_macros_noalloc.argtypes = [_vp, _dp, _dp, _dp]
+    L.lbgpu_moments.argtypes = [_vp, _dp]
+    L.lbgpu_velocity_accumulate.argtypes = [_vp]
+    L.lbgpu_velocity_average.argtypes = [_vp, _dp, _dp, ctypes.POINTER(ctypes.c_longlong)]
+    L.lbgpu_velocity_reset.argtypes = [_vp]
     L.lbgpu_synchronize.argtypes = [_vp]
     L.lbgpu_stream.restype = _vp
     L.lbgpu_stream.argtypes = [_vp]
@@ -209,6 +213,25 @@ class Lattice:
         _check(lib().lbgpu_get_macros_noalloc(self.h, _p(rho), _p(ux), _p(uy)))
         shp = (self.ly, self.lx)
         return rho.reshape(shp), ux.reshape(shp), uy.reshape(shp)
+
+    def moments(self):
+        """FP64 sums: mass, jx, jy, Fx, Fy, kinetic energy, non-finite nodes, bulk mass."""
+        out = np.zeros(8)
+        _check(lib().lbgpu_moments(self.h, _p(out)))
+        return out
+
+    def velocity_accumulate(self):
+        _check(lib().lbgpu_velocity_accumulate(self.h))
+
+    def velocity_average(self):
+        n = self.lx * self.ly
+        ux, uy = np.zeros(n), np.zeros(n)
+        k = ctypes.c_longlong()
+        _check(lib().lbgpu_velocity_average(self.h, _p(ux), _p(uy), ctypes.byref(k)))
+        return ux.reshape(self.ly, self.lx), uy.reshape(self.ly, self.lx), k.value
+
+    def velocity_reset(self):
+        _check(lib().lbgpu_velocity_reset(self.h))
 
     @property
     def stream(self):

@@ -275,6 +275,43 @@ int orc_run(int lx, int ly, double omega, const unsigned char *tag, double *bc,
     return 0;
 }
 
+/* Sums of a lattice state, the checker of the GPU reductions (no reference counterpart: the
+ * reference computes no forces).  out[0] mass, [1..2] momentum, [3..4] momentum-exchange force
+ * on bounce-back nodes strictly inside the lattice (2 c_i f_i over links entering them from
+ * non-bounce-back nodes), [5] kinetic energy |j|^2/(2 rho) of BGK nodes, [6] nodes with a
+ * non-finite population, [7] mass of BGK nodes.  Plain left-to-right sums. */
+void orc_moments(int lx, int ly, const unsigned char *tag, const double *lat, double *out)
+{
+    const int ny2 = ly + 2;
+    int X, Y, i, k;
+    for (k = 0; k < 8; ++k) out[k] = 0.;
+    for (X = 1; X <= lx; ++X)
+        for (Y = 1; Y <= ly; ++Y) {
+            const double *f = &lat[((size_t)X * ny2 + Y) * 9];
+            double rho = 0., jx = 0., jy = 0.;
+            int bad = 0;
+            for (i = 0; i < 9; ++i) {
+                rho += f[i];
+                jx += CX[i] * f[i];
+                jy += CY[i] * f[i];
+                bad |= !(f[i] - f[i] == 0.);
+            }
+            out[0] += rho; out[1] += jx; out[2] += jy;
+            out[6] += bad ? 1. : 0.;
+            if (tag[X * ny2 + Y] == ORC_BGK) {
+                out[5] += (jx * jx + jy * jy) / (2. * rho);
+                out[7] += rho;
+            } else if (tag[X * ny2 + Y] == ORC_BOUNCE_BACK && X >= 2 && X <= lx - 1 && Y >= 2 &&
+                       Y <= ly - 1) {
+                for (i = 1; i < 9; ++i)
+                    if (tag[(X - CX[i]) * ny2 + (Y - CY[i])] != ORC_BOUNCE_BACK) {
+                        out[3] += 2. * CX[i] * f[i];
+                        out[4] += 2. * CY[i] * f[i];
+                    }
+            }
+        }
+}
+
 /* Poiseuille profile of the application driver (unsteady.c:155-159). */
 static double poiseuille(int iY, int ly, double uMax)
 {

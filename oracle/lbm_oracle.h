@@ -51,6 +51,10 @@ double orc_equilibrium(int i, double rho, double ux, double uy, double usqr);
 void orc_collide_node(int tag, double *f, double omega, const double *param2);
 void orc_init_equilibrium(double *f, double rho, double ux, double uy);
 
+/* Sums of a state (mass, momentum, obstacle force, kinetic energy, non-finite nodes, bulk
+ * mass) -- the checker of the GPU reductions; see lbm_oracle.c. */
+void orc_moments(int lx, int ly, const unsigned char *tag, const double *lat, double *out);
+
 /* Cylinder geometry builder used by the tests (the application driver's iniGeometry,
  * unsteady.c:162-199, with the wall/outlet options of the harness).  Fills tag, bc,
  * zgb_row and the initial populations of lat; tmp is zeroed.  Returns omega. */

@@ -86,6 +86,7 @@ def oracle_lib():
         lib.orc_equilibrium.argtypes = [ctypes.c_int] + [ctypes.c_double] * 4
         lib.orc_collide_node.argtypes = [ctypes.c_int, _dp, ctypes.c_double, _dp]
         lib.orc_init_equilibrium.argtypes = [_dp] + [ctypes.c_double] * 3
+        lib.orc_moments.argtypes = [ctypes.c_int, ctypes.c_int, _u8p, _dp, _dp]
         _ORACLE = lib
     return _ORACLE
 
@@ -257,3 +258,12 @@ def random_boundary_lattice(lx, ly, seed, omega=1.6, kinds="mixed"):
             tmp[X, Y] = f * (1 + rng.uniform(-0.01, 0.01, 9))
     zgb = np.zeros(ly + 2, np.uint8)
     return OracleState(lx, ly, omega, tag, bc.reshape(-1), zgb, lat, tmp)
+
+
+def moments(state: OracleState):
+    """orc_moments of a state: mass, jx, jy, Fx, Fy, kinetic energy, non-finite nodes, bulk mass."""
+    tag = np.ascontiguousarray(state.tag.reshape(-1), np.uint8)
+    lat = np.ascontiguousarray(state.lat.reshape(-1))
+    out = np.zeros(8)
+    oracle_lib().orc_moments(state.lx, state.ly, _ptr(tag, _u8p), _ptr(lat), _ptr(out))
+    return out
