@@ -278,9 +278,9 @@ def time_lattice(lbgpu, nx, ny, precision, scheme, steps, warmup, dist, sampler_
     ox, oy, r = cylinder(nx, ny)
     lat = lbgpu.Lattice(nx, ny, precision, scheme)
     try:
-        lat.setup_cylinder(ox, oy, r, 0.02, 100.0, lbgpu.WALL_BOUNCEBACK, lbgpu.OUTLET_CONST)
-        if precision in ("f16", "bf16"):
+        if precision in ("f16", "bf16"):   # the scale encodes the initial state: set it first
             lat.set_offset_scale(lbgpu_default_scale(precision))
+        lat.setup_cylinder(ox, oy, r, 0.02, 100.0, lbgpu.WALL_BOUNCEBACK, lbgpu.OUTLET_CONST)
         lat.step(warmup)
         lat.synchronize()
         dist.barrier()

@@ -169,6 +169,42 @@ int lbgpu_velocity_average(lbgpu_lattice *lat, double *ux, double *uy, long long
 int lbgpu_velocity_reset(lbgpu_lattice *lat);
 
 int lbgpu_synchronize(lbgpu_lattice *lat);
+
+/* ---- batches: many independent lattices in one launch per step --------------------------
+ * No counterpart in the reference (one lattice per process).  Members are lattices of the
+ * batch's precision, pull or AA, with constant-density outlets (an extrapolated outlet is
+ * stepped on its own).  lbgpu_batch_step advances every member by nsteps: one persistent
+ * launch per step and scheme walks a work list of tiles; chunks of 50 steps are replayed as a
+ * CUDA graph.  Each member's result is bit-identical to stepping it alone.  The batch does not
+ * own its members; remove a member before destroying it.  Steps are asynchronous on the batch's
+ * stream and ordered with the members' own streams. */
+typedef struct lbgpu_batch lbgpu_batch;
+int lbgpu_batch_create(int precision, lbgpu_batch **out);
+int lbgpu_batch_destroy(lbgpu_batch *b);
+int lbgpu_batch_add(lbgpu_batch *b, lbgpu_lattice *lat, int *slot);
+int lbgpu_batch_remove(lbgpu_batch *b, int slot);
+int lbgpu_batch_size(lbgpu_batch *b);
+int lbgpu_batch_step(lbgpu_batch *b, int nsteps);
+int lbgpu_batch_step_timed(lbgpu_batch *b, int nsteps, float *ms);
+int lbgpu_batch_synchronize(lbgpu_batch *b);
+int lbgpu_batch_last_launches(lbgpu_batch *b);
+
+/* Tile shape of a size class (class of a lattice = lbgpu_batch_size_class(lx*ly), 0..5 for
+ * < 16K, 64K, 256K, 1M, 4M nodes and above): tiles tile_width (32, 64, 128) nodes wide,
+ * each of the 128 threads doing rows_per_thread (1, 2, 4) nodes down y. */
+int lbgpu_batch_size_class(long long nodes);
+int lbgpu_batch_set_shape(lbgpu_batch *b, int size_class, int tile_width, int rows_per_thread);
+int lbgpu_batch_get_shape(lbgpu_batch *b, int size_class, int *tile_width, int *rows_per_thread);
+
+/* Autotuner: for each size class present, time `steps` batch steps with each of the nine tile
+ * shapes and keep the fastest (the members really advance 9 x steps per class); best_ms[6]
+ * receives each class's best time when not NULL. */
+int lbgpu_batch_autotune(lbgpu_batch *b, int steps, float *best_ms);
+
+/* Autotuner for the scheme: time a cylinder channel of lx x ly in the pull and the AA scheme
+ * and return the faster one (*scheme), with both timings for `steps` steps. */
+int lbgpu_tune_scheme(int precision, int lx, int ly, int steps, int *scheme, float *ms_pull,
+                      float *ms_aa);
 void *lbgpu_stream(lbgpu_lattice *lat);           /* the lattice's cudaStream_t            */
 long long lbgpu_steps_done(lbgpu_lattice *lat);
 size_t lbgpu_device_bytes(lbgpu_lattice *lat);     /* device memory held by the lattice     */

@@ -402,18 +402,13 @@ __global__ void __launch_bounds__(BX) k_stream(Geo g, const S *__restrict__ src,
 
 // ---- AA scheme ----------------------------------------------------------------------------
 
-// Even step: own natural slots (stale ones from the side store) -> collide -> own opposite slots.
+// Even step at node (X, Y): own natural slots (stale ones from the side store) -> collide ->
+// own opposite slots.
 template <class S>
-__global__ void __launch_bounds__(BX) k_aa_even(Geo g, S *__restrict__ a,
-                                                const uint8_t *__restrict__ tag,
-                                                const double *__restrict__ bc, double omega,
-                                                S *__restrict__ side, float sc, float inv)
+__device__ __forceinline__ void aa_even_node(const Geo &g, S *__restrict__ a, const uint8_t *__restrict__ tag,
+                                             const double *__restrict__ bc, double omega,
+                                             S *__restrict__ side, float sc, float inv, int X, int Y)
 {
-    using C = Codec<S>;
-    using R = typename C::R;
-    const int X = blockIdx.x * BX + threadIdx.x + 1;
-    const int Y = blockIdx.y + 1;
-    if (X > g.lx) return;
     const long long o = g.idx(X, Y);
     const bool edge = g.perimeter(X, Y);
     const int p = edge ? g.pidx(X, Y) : 0;
@@ -433,22 +428,16 @@ __global__ void __launch_bounds__(BX) k_aa_even(Geo g, S *__restrict__ a,
     }
 }
 
-// Odd step: gather direction i from the source neighbour's opposite slot (stale slots from the
-// side store) -> collide -> scatter direction i to the destination neighbour's natural slot.
-// Slot A[i][x + c_i] is read (as opp of the neighbour's gather) and written by the same thread,
-// so the in-place update is race-free.  Destinations in the ghost ring are written too, so the
-// natural form carries the values streamed out of the lattice.
+// Odd step at node (X, Y): gather direction i from the source neighbour's opposite slot (stale
+// slots from the side store) -> collide -> scatter direction i to the destination neighbour's
+// natural slot.  Slot A[i][x + c_i] is read (as opp of the neighbour's gather) and written by
+// the same thread, so the in-place update is race-free.  Destinations in the ghost ring are
+// written too, so the natural form carries the values streamed out of the lattice.
 template <class S>
-__global__ void __launch_bounds__(BX) k_aa_odd(Geo g, S *__restrict__ a,
-                                               const uint8_t *__restrict__ tag,
-                                               const double *__restrict__ bc, double omega,
-                                               S *__restrict__ side, float sc, float inv)
+__device__ __forceinline__ void aa_odd_node(const Geo &g, S *__restrict__ a, const uint8_t *__restrict__ tag,
+                                            const double *__restrict__ bc, double omega,
+                                            S *__restrict__ side, float sc, float inv, int X, int Y)
 {
-    using C = Codec<S>;
-    using R = typename C::R;
-    const int X = blockIdx.x * BX + threadIdx.x + 1;
-    const int Y = blockIdx.y + 1;
-    if (X > g.lx) return;
     const long long o = g.idx(X, Y);
     const bool edge = g.perimeter(X, Y);
     const int p = edge ? g.pidx(X, Y) : 0;
@@ -462,7 +451,7 @@ __global__ void __launch_bounds__(BX) k_aa_odd(Geo g, S *__restrict__ a,
         for (int i = 0; i < 9; ++i) {
             const int sx = X - cx(i), sy = Y - cy(i);
             f[i] = Work<S>::load(g.interior(sx, sy) ? plane(a, g, opp(i))[g.idx(sx, sy)]
-                                             : side[(size_t)i * g.nper + p], i, inv);
+                                                    : side[(size_t)i * g.nper + p], i, inv);
         }
     }
     collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
@@ -473,6 +462,74 @@ __global__ void __launch_bounds__(BX) k_aa_odd(Geo g, S *__restrict__ a,
 #pragma unroll
         for (int i = 0; i < 9; ++i)
             if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
+    }
+}
+
+template <class S>
+__global__ void __launch_bounds__(BX) k_aa_even(Geo g, S *__restrict__ a,
+                                                const uint8_t *__restrict__ tag,
+                                                const double *__restrict__ bc, double omega,
+                                                S *__restrict__ side, float sc, float inv)
+{
+    const int X = blockIdx.x * BX + threadIdx.x + 1;
+    const int Y = blockIdx.y + 1;
+    if (X <= g.lx) aa_even_node<S>(g, a, tag, bc, omega, side, sc, inv, X, Y);
+}
+
+template <class S>
+__global__ void __launch_bounds__(BX) k_aa_odd(Geo g, S *__restrict__ a,
+                                               const uint8_t *__restrict__ tag,
+                                               const double *__restrict__ bc, double omega,
+                                               S *__restrict__ side, float sc, float inv)
+{
+    const int X = blockIdx.x * BX + threadIdx.x + 1;
+    const int Y = blockIdx.y + 1;
+    if (X <= g.lx) aa_odd_node<S>(g, a, tag, bc, omega, side, sc, inv, X, Y);
+}
+
+// ---- many lattices in one launch ----------------------------------------------------------
+//
+// One time step of every lattice of a batch: a fixed grid of blocks walks a work list of tiles
+// (lattice, x0, y0, shape).  A tile is `tw` = 32 << (shape & 3) nodes wide and (128 / tw) << r
+// rows high (r = shape >> 2), one block of 128 threads, each thread doing 1 << r nodes down y.
+// A lattice's buffers and parities at step k of a chunk follow from its state at the chunk's
+// start (BatchInst), so a CUDA graph of the chunk's launches replays unchanged.  Each node runs
+// the same function as the single-lattice kernels, so a lattice's result is the same in the
+// batch and alone.
+template <class S, bool AA>
+__global__ void __launch_bounds__(BATCH_THREADS) k_batch(const BatchInst *__restrict__ insts,
+                                                         const BatchWork *__restrict__ work,
+                                                         const int *__restrict__ nwork_p, int k)
+{
+    const int nwork = *nwork_p;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const BatchWork it = work[w];
+        const BatchInst &d = insts[it.inst];
+        const Geo g = d.g;
+        const int tw = 32 << (it.shape & 3);
+        const int r = it.shape >> 2;
+        const int dx = threadIdx.x & (tw - 1);
+        const int rows = 1 << r;
+        const int dy0 = (threadIdx.x / tw) << r;
+        const int X = it.x0 + dx;
+        if (X > g.lx) continue;
+        const int tau = d.tau0 + k;
+        S *side = static_cast<S *>(d.side) + (size_t)(tau & 1) * 9 * (size_t)g.nper;
+        for (int j = 0; j < rows; ++j) {
+            const int Y = it.y0 + dy0 + j;
+            if (Y > g.ly) break;
+            if (!AA) {
+                const int src = d.cur0 ^ (k & 1);
+                pull_node<S>(g, static_cast<const S *>(d.buf[src]), static_cast<S *>(d.buf[src ^ 1]),
+                             d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, X, Y);
+            } else if (((d.phase0 + k) & 1) == 0) {
+                aa_even_node<S>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, d.omega, side,
+                                d.scale, d.inv_scale, X, Y);
+            } else {
+                aa_odd_node<S>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, d.omega, side,
+                               d.scale, d.inv_scale, X, Y);
+            }
+        }
     }
 }
 
@@ -837,6 +894,46 @@ void launch_aa_odd(const DevLattice &d, int side_par, cudaStream_t s)
     dim3 grid(cdiv(d.g.lx, BX), d.g.ly);
     LBGPU_DISPATCH(d, (k_aa_odd<S><<<grid, BX, 0, s>>>(d.g, B<S>(d, 0), d.tag, d.bc, d.omega,
                        SIDE<S>(d, side_par), d.scale, d.inv_scale)));
+}
+
+template <class S>
+static void launch_batch_t(int scheme, const BatchInst *insts, const BatchWork *work, const int *nwork,
+                           int grid, int k, cudaStream_t s)
+{
+    if (scheme == LBGPU_AA) k_batch<S, true><<<grid, BATCH_THREADS, 0, s>>>(insts, work, nwork, k);
+    else k_batch<S, false><<<grid, BATCH_THREADS, 0, s>>>(insts, work, nwork, k);
+}
+
+void launch_batch(int precision, int scheme, const BatchInst *insts, const BatchWork *work,
+                  const int *nwork, int grid, int k, cudaStream_t s)
+{
+    switch (precision) {
+    case LBGPU_F64: launch_batch_t<double>(scheme, insts, work, nwork, grid, k, s); break;
+    case LBGPU_F32: launch_batch_t<float>(scheme, insts, work, nwork, grid, k, s); break;
+    case LBGPU_F16: launch_batch_t<__half>(scheme, insts, work, nwork, grid, k, s); break;
+    default: launch_batch_t<__nv_bfloat16>(scheme, insts, work, nwork, grid, k, s); break;
+    }
+}
+
+template <class S>
+static int blocks_t(int scheme)
+{
+    int n = 0;
+    if (scheme == LBGPU_AA)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch<S, true>, BATCH_THREADS, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch<S, false>, BATCH_THREADS, 0);
+    return n;
+}
+
+int batch_blocks_per_sm(int precision, int scheme)
+{
+    switch (precision) {
+    case LBGPU_F64: return blocks_t<double>(scheme);
+    case LBGPU_F32: return blocks_t<float>(scheme);
+    case LBGPU_F16: return blocks_t<__half>(scheme);
+    default: return blocks_t<__nv_bfloat16>(scheme);
+    }
 }
 
 void launch_side_from_buf(const DevLattice &d, int b, int side_par, cudaStream_t s)

@@ -51,6 +51,35 @@ void launch_moments(const DevLattice &d, int view, int cur, int side_par, double
 // acc[0..lx*ly) += ux, acc[lx*ly..2*lx*ly) += uy of the current state.
 void launch_accumulate_velocity(const DevLattice &d, int view, int cur, int side_par, double *acc,
                                 cudaStream_t s);
+// ---- batches: many lattices per launch ------------------------------------------------
+constexpr int BATCH_THREADS = 128;
+
+// One lattice of a batch, with its state at the start of the current chunk of steps:
+// pull scheme: the buffer holding C_n is buf[cur0]; AA: phase0 0 = natural form, 1 = swapped;
+// tau0 = the time step the chunk's first launch executes (its side parity is tau0 & 1).
+struct BatchInst {
+    Geo g;
+    void *buf[2];
+    void *side;
+    const uint8_t *tag;
+    const double *bc;
+    double omega;
+    float scale, inv_scale;
+    int scheme, cur0, phase0, tau0;
+};
+
+// A tile of a lattice: nodes x0 .. x0 + tw - 1 and y0 .. y0 + (128/tw << r) - 1,
+// tw = 32 << (shape & 3), r = shape >> 2.
+struct BatchWork {
+    int inst, x0, y0, shape;
+};
+
+// Step k of a chunk for every lattice of one scheme in the batch; `grid` blocks walk the work
+// list (one list per scheme, each kernel specialised for its scheme).
+void launch_batch(int precision, int scheme, const BatchInst *insts, const BatchWork *work,
+                  const int *nwork, int grid, int k, cudaStream_t s);
+int batch_blocks_per_sm(int precision, int scheme);
+
 // AA scheme (buffer 0): the even step collides every node in place into the opposite slots,
 // the odd step gathers from the neighbours' opposite slots and scatters to their natural slots.
 void launch_aa_even(const DevLattice &d, int side_par, cudaStream_t s);

@@ -83,6 +83,23 @@ def lib():
     L.lbgpu_velocity_average.argtypes = [_vp, _dp, _dp, ctypes.POINTER(ctypes.c_longlong)]
     L.lbgpu_velocity_reset.argtypes = [_vp]
     L.lbgpu_synchronize.argtypes = [_vp]
+    L.lbgpu_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(_vp)]
+    L.lbgpu_batch_destroy.argtypes = [_vp]
+    L.lbgpu_batch_add.argtypes = [_vp, _vp, ctypes.POINTER(ctypes.c_int)]
+    L.lbgpu_batch_remove.argtypes = [_vp, ctypes.c_int]
+    L.lbgpu_batch_size.argtypes = [_vp]
+    L.lbgpu_batch_step.argtypes = [_vp, ctypes.c_int]
+    L.lbgpu_batch_step_timed.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    L.lbgpu_batch_synchronize.argtypes = [_vp]
+    L.lbgpu_batch_last_launches.argtypes = [_vp]
+    L.lbgpu_batch_size_class.argtypes = [ctypes.c_longlong]
+    L.lbgpu_batch_set_shape.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.lbgpu_batch_get_shape.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int)]
+    L.lbgpu_batch_autotune.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    L.lbgpu_tune_scheme.argtypes = [ctypes.c_int] * 4 + [ctypes.POINTER(ctypes.c_int),
+                                                         ctypes.POINTER(ctypes.c_float),
+                                                         ctypes.POINTER(ctypes.c_float)]
     L.lbgpu_stream.restype = _vp
     L.lbgpu_stream.argtypes = [_vp]
     L.lbgpu_steps_done.restype = ctypes.c_longlong
@@ -250,11 +267,17 @@ class Lattice:
         return lib().lbgpu_last_kernel_launches(self.h)
 
 
+DEFAULT_SCALE = {"f16": 10, "bf16": 6}
+
+
 def cylinder_lattice(lx, ly, precision="f64", scheme="pull", umax=0.02, re=100.0,
-                     wall=WALL_BOUNCEBACK, outlet=OUTLET_CONST, obst=None):
-    """A device lattice holding the channel (obstacle default (lx/5+1, ly/2+1), r = ly/10+1)."""
+                     wall=WALL_BOUNCEBACK, outlet=OUTLET_CONST, obst=None, scale=None):
+    """A device lattice holding the channel (obstacle default (lx/5+1, ly/2+1), r = ly/10+1).
+    16-bit storage uses the offset scale 2^scale (default DEFAULT_SCALE)."""
     ox, oy, r = obst if obst is not None else (lx // 5 + 1, ly // 2 + 1, ly // 10 + 1)
     lat = Lattice(lx, ly, precision, scheme)
+    if precision in DEFAULT_SCALE:
+        lat.set_offset_scale(DEFAULT_SCALE[precision] if scale is None else scale)
     lat.omega = lat.setup_cylinder(ox, oy, r, umax, re, wall, outlet)
     return lat
 
@@ -295,3 +318,78 @@ def declared_functions():
             if m and m.group(1) not in ("if", "for", "while", "switch"):
                 names.add(m.group(1))
     return sorted(names)
+
+
+class Batch:
+    """lbgpu_batch: many lattices of one precision stepped together (one launch per step)."""
+
+    def __init__(self, precision="f32"):
+        self.precision = precision
+        h = _vp()
+        _check(lib().lbgpu_batch_create(PRECISIONS[precision], ctypes.byref(h)))
+        self.h = h
+        self.members = {}
+
+    def close(self):
+        if self.h:
+            lib().lbgpu_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add(self, lat):
+        slot = ctypes.c_int()
+        _check(lib().lbgpu_batch_add(self.h, lat.h, ctypes.byref(slot)))
+        self.members[slot.value] = lat
+        return slot.value
+
+    def remove(self, slot):
+        _check(lib().lbgpu_batch_remove(self.h, int(slot)))
+        self.members.pop(slot, None)
+
+    def __len__(self):
+        return lib().lbgpu_batch_size(self.h)
+
+    def step(self, n):
+        _check(lib().lbgpu_batch_step(self.h, int(n)))
+
+    def step_timed(self, n):
+        ms = ctypes.c_float()
+        _check(lib().lbgpu_batch_step_timed(self.h, int(n), ctypes.byref(ms)))
+        return ms.value
+
+    def synchronize(self):
+        _check(lib().lbgpu_batch_synchronize(self.h))
+
+    @property
+    def last_launches(self):
+        return lib().lbgpu_batch_last_launches(self.h)
+
+    def set_shape(self, size_class, tile_width, rows_per_thread):
+        _check(lib().lbgpu_batch_set_shape(self.h, size_class, tile_width, rows_per_thread))
+
+    def shape(self, size_class):
+        w, r = ctypes.c_int(), ctypes.c_int()
+        _check(lib().lbgpu_batch_get_shape(self.h, size_class, ctypes.byref(w), ctypes.byref(r)))
+        return w.value, r.value
+
+    def autotune(self, steps=4):
+        best = (ctypes.c_float * 6)()
+        _check(lib().lbgpu_batch_autotune(self.h, int(steps), best))
+        return list(best)
+
+
+def size_class(nodes):
+    return lib().lbgpu_batch_size_class(int(nodes))
+
+
+def tune_scheme(precision, lx, ly, steps=10):
+    """(scheme name, ms pull, ms aa) for a channel of lx x ly."""
+    s, a, b = ctypes.c_int(), ctypes.c_float(), ctypes.c_float()
+    _check(lib().lbgpu_tune_scheme(PRECISIONS[precision], lx, ly, steps, ctypes.byref(s),
+                                   ctypes.byref(a), ctypes.byref(b)))
+    return ("aa" if s.value == 1 else "pull"), a.value, b.value

@@ -1,0 +1,115 @@
+"""Batches: many lattices of uneven size in one launch per step (lbgpu_batch_*).
+
+The contract: every member's populations after a batch step are bit-identical to the same
+lattice stepped alone, for both schemes and every precision, across chunk boundaries (CUDA-graph
+replays of 50 steps), odd remainders, membership changes and autotuned tile shapes.
+"""
+import numpy as np
+import pytest
+
+import lbgpu
+from helpers import describe_diff, same
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(96, 40), (200, 64), (64, 33), (130, 50), (257, 35), (33, 96)]
+
+
+def channel(lx, ly, precision, scheme, seed):
+    rng = np.random.default_rng(seed)
+    r = max(2, int(round(ly / 10 * rng.uniform(0.8, 1.2))))
+    ox = int(lx / 5 * rng.uniform(0.9, 1.1)) + 1
+    oy = int(ly / 2 * rng.uniform(0.9, 1.1)) + 1
+    lat = lbgpu.Lattice(lx, ly, precision, scheme)
+    if precision in ("f16", "bf16"):
+        lat.set_offset_scale(10 if precision == "f16" else 6)
+    lat.setup_cylinder(ox, oy, r, rng.uniform(0.01, 0.04), rng.uniform(20, 200),
+                       lbgpu.WALL_BOUNCEBACK, lbgpu.OUTLET_CONST)
+    return lat
+
+
+def alone(lx, ly, precision, scheme, seed, steps):
+    with channel(lx, ly, precision, scheme, seed) as lat:
+        lat.step(steps)
+        return lat.populations()
+
+
+@pytest.mark.parametrize("precision", ["f32", "f16", "f64"])
+def test_members_match_lattices_stepped_alone(precision):
+    schemes = ["pull", "aa", "pull", "aa", "pull", "aa"]
+    lats = [channel(lx, ly, precision, s, k) for k, ((lx, ly), s) in enumerate(zip(SIZES, schemes))]
+    with lbgpu.Batch(precision) as b:
+        slots = [b.add(l) for l in lats]
+        assert len(b) == len(lats)
+        for n in (3, 50, 84):          # a prologue step, a full graph chunk, chunk + odd rest
+            b.step(n)
+        b.synchronize()
+        got = [l.populations() for l in lats]
+        assert all(l.steps_done == 137 for l in lats)
+        for s in slots:
+            b.remove(s)
+    for k, ((lx, ly), s) in enumerate(zip(SIZES, schemes)):
+        exp = alone(lx, ly, precision, s, k, 137)
+        assert same(got[k], exp), (precision, k, s, describe_diff(got[k], exp))
+    for l in lats:
+        l.close()
+
+
+def test_membership_changes_between_steps():
+    lats = [channel(lx, ly, "f32", "pull", k) for k, (lx, ly) in enumerate(SIZES[:4])]
+    with lbgpu.Batch("f32") as b:
+        slots = [b.add(l) for l in lats]
+        b.step(20)
+        b.remove(slots[1])
+        newcomer = channel(70, 45, "f32", "aa", 99)
+        b.add(newcomer)
+        b.step(61)
+        b.synchronize()
+        got = [l.populations() for l in lats] + [newcomer.populations()]
+        for s in list(b.members):
+            b.remove(s)
+    assert same(got[0], alone(*SIZES[0], "f32", "pull", 0, 81))
+    assert same(got[1], alone(*SIZES[1], "f32", "pull", 1, 20))
+    assert same(got[2], alone(*SIZES[2], "f32", "pull", 2, 81))
+    assert same(got[4], alone(70, 45, "f32", "aa", 99, 61))
+    for l in lats + [newcomer]:
+        l.close()
+
+
+def test_autotuned_shapes_keep_results_exact():
+    lats = [channel(lx, ly, "f32", "pull", k) for k, (lx, ly) in enumerate(SIZES[:3])]
+    with lbgpu.Batch("f32") as b:
+        slots = [b.add(l) for l in lats]
+        best = b.autotune(2)
+        classes = {lbgpu.size_class(lx * ly) for lx, ly in SIZES[:3]}
+        for c in classes:
+            w, r = b.shape(c)
+            assert w in (32, 64, 128) and r in (1, 2, 4)
+            assert best[c] > 0
+        b.step(7)
+        b.synchronize()
+        got = [(l.populations(), l.steps_done) for l in lats]
+        for s in slots:
+            b.remove(s)
+    for k, (lx, ly) in enumerate(SIZES[:3]):
+        pops, steps = got[k]
+        assert same(pops, alone(lx, ly, "f32", "pull", k, steps)), k
+    for l in lats:
+        l.close()
+
+
+def test_batch_rejects_mismatched_members():
+    with lbgpu.Batch("f32") as b, lbgpu.Lattice(40, 20, "f64") as wrong:
+        with pytest.raises(lbgpu.LbError) as e:
+            b.add(wrong)
+        assert e.value.code == 3
+    with lbgpu.Batch("f64") as b, lbgpu.Lattice(40, 20, "f64") as zgb:
+        zgb.setup_cylinder(9, 11, 3, 0.02, 100.0, lbgpu.WALL_REGULARIZED, lbgpu.OUTLET_ZGB)
+        with pytest.raises(lbgpu.LbError) as e:
+            b.add(zgb)
+        assert e.value.code == 3
+
+
+def test_scheme_tuner_reports_both_timings():
+    scheme, t_pull, t_aa = lbgpu.tune_scheme("f32", 512, 128, 6)
+    assert scheme in ("pull", "aa") and t_pull > 0 and t_aa > 0
