@@ -56,6 +56,10 @@ def parse():
     p.add_argument("--scheme", default="pull", choices=["pull", "aa"])
     p.add_argument("--variants", default="auto",
                    help="comma list of precision:scheme also timed, 'auto' or 'none'")
+    p.add_argument("--study", choices=["batching", "serving", "precision"], default=None,
+                   help="run a workload study instead of the headline benchmark (one GPU)")
+    p.add_argument("--study-args", default="",
+                   help="comma-separated key=value overrides of the study's defaults")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=20.0,
@@ -395,11 +399,44 @@ def run_ours(args, dist):
         print(json.dumps(line))
 
 
+def run_study(args, dist):
+    """One study on this rank's GPU (rank 0 prints; the studies are single-GPU workloads)."""
+    import lbgpu
+    import studies
+
+    rc = lbgpu.lib().lbgpu_set_device(dist.local)
+    if rc != 0:
+        raise lbgpu.LbError(rc, lbgpu.last_error()[1])
+    kw = {}
+    for item in filter(None, args.study_args.split(",")):
+        k, v = item.split("=", 1)
+        if "/" in v or k in ("precisions", "cases"):
+            kw[k] = tuple(v.split("/"))
+        else:
+            try:
+                kw[k] = int(v)
+            except ValueError:
+                kw[k] = float(v) if v.replace(".", "", 1).replace("e-", "", 1).isdigit() else v
+    if dist.rank != 0:
+        return
+    fn = {"batching": studies.batching_study, "serving": studies.serving_study,
+          "precision": studies.precision_study}[args.study]
+    t0 = time.time()
+    with ClockSampler(dist.local) as cs:
+        res = fn(**kw)
+    res = {"study": args.study, "args": {k: list(v) if isinstance(v, tuple) else v
+                                         for k, v in kw.items()},
+           "wall_s": round(time.time() - t0, 1), "clocks": cs.summary(), **res}
+    print(json.dumps(res))
+
+
 def main():
     args = parse()
     dist = Dist()
     try:
-        if args.impl == "reference":
+        if args.study:
+            run_study(args, dist)
+        elif args.impl == "reference":
             run_reference_arm(args, dist)
         else:
             run_ours(args, dist)

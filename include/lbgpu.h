@@ -173,9 +173,9 @@ int lbgpu_synchronize(lbgpu_lattice *lat);
 /* ---- batches: many independent lattices in one launch per step --------------------------
  * No counterpart in the reference (one lattice per process).  Members are lattices of the
  * batch's precision, pull or AA, with constant-density outlets (an extrapolated outlet is
- * stepped on its own).  lbgpu_batch_step advances every member by nsteps: one persistent
- * launch per step and scheme walks a work list of tiles; chunks of 50 steps are replayed as a
- * CUDA graph.  Each member's result is bit-identical to stepping it alone.  The batch does not
+ * stepped on its own).  lbgpu_batch_step advances every member by nsteps: per step one launch
+ * for the pull members and one for each phase of the AA members walks a work list of 128-node
+ * tiles; chunks of 50 steps are replayed as a CUDA graph.  Each member's result is bit-identical to stepping it alone.  The batch does not
  * own its members; remove a member before destroying it.  Steps are asynchronous on the batch's
  * stream and ordered with the members' own streams. */
 typedef struct lbgpu_batch lbgpu_batch;
@@ -190,19 +190,75 @@ int lbgpu_batch_synchronize(lbgpu_batch *b);
 int lbgpu_batch_last_launches(lbgpu_batch *b);
 
 /* Tile shape of a size class (class of a lattice = lbgpu_batch_size_class(lx*ly), 0..5 for
- * < 16K, 64K, 256K, 1M, 4M nodes and above): tiles tile_width (32, 64, 128) nodes wide,
- * each of the 128 threads doing rows_per_thread (1, 2, 4) nodes down y. */
+ * < 16K, 64K, 256K, 1M, 4M nodes and above): nodes_per_thread 1: tiles tile_width (32, 64,
+ * 128) nodes wide and threads / tile_width rows high, one node per thread of a block of
+ * `threads` threads; nodes_per_thread 4 (16-bit storage, tile_width 128, pull members): each
+ * warp one row of 128 nodes, four per thread.  Defaults: 128 wide, one node per thread; four
+ * nodes per thread for 16-bit lattices of 64K nodes and more. */
 int lbgpu_batch_size_class(long long nodes);
-int lbgpu_batch_set_shape(lbgpu_batch *b, int size_class, int tile_width, int rows_per_thread);
-int lbgpu_batch_get_shape(lbgpu_batch *b, int size_class, int *tile_width, int *rows_per_thread);
+int lbgpu_batch_set_shape(lbgpu_batch *b, int size_class, int tile_width, int nodes_per_thread);
+int lbgpu_batch_get_shape(lbgpu_batch *b, int size_class, int *tile_width, int *nodes_per_thread);
+/* Launch form: 1 = a persistent grid (resident blocks per SM x SMs) strides through the work
+ * list (the default), 0 = one block per tile. */
+int lbgpu_batch_set_persistent(lbgpu_batch *b, int persistent);
+int lbgpu_batch_get_persistent(lbgpu_batch *b);
+/* Threads per tile (= nodes per tile, one block per tile): 128 (default), 256 or 512. */
+int lbgpu_batch_set_threads(lbgpu_batch *b, int threads);
+int lbgpu_batch_get_threads(lbgpu_batch *b);
 
-/* Autotuner: for each size class present, time `steps` batch steps with each of the nine tile
- * shapes and keep the fastest (the members really advance 9 x steps per class); best_ms[6]
- * receives each class's best time when not NULL. */
+/* Autotuner: times `steps` batch steps (after one untimed step) with each threads-per-tile and
+ * launch-form pair, then, for each size class present, with each tile shape (three widths, and
+ * four nodes per thread for 16-bit storage), keeping the fastest at each stage (the members
+ * really advance 6 x (steps + 1) plus 3 or 4 x (steps + 1) per class present); best_ms[6]
+ * receives each class's best time (0 for classes not present) when not NULL. */
 int lbgpu_batch_autotune(lbgpu_batch *b, int steps, float *best_ms);
 
-/* Autotuner for the scheme: time a cylinder channel of lx x ly in the pull and the AA scheme
- * and return the faster one (*scheme), with both timings for `steps` steps. */
+/* Device bytes a lattice of this size, precision and scheme allocates. */
+size_t lbgpu_lattice_bytes(int lx, int ly, int precision, int scheme);
+
+/* ---- serving: continuous batching of simulation requests --------------------------------
+ * No counterpart in the reference.  A request is a cylinder channel (bounce-back walls,
+ * constant-density outlet) with a step cap (a multiple of the server's check interval) and a
+ * steady-state tolerance: it retires when the largest velocity change over one check interval
+ * falls below `tol` (0: never) or at the cap; a request whose velocity becomes non-finite
+ * retires at that check with converged = -1.  lbgpu_server_run serves every submitted request,
+ * honouring arrival times (seconds after the run starts) in wall-clock time: batched = 1 admits
+ * requests in arrival order while their lattices fit the budget and steps all resident ones
+ * together (lbgpu_batch); batched = 0 solves them one at a time on their own (plain solves). */
+typedef struct {
+    int lx, ly, obst_x, obst_y, obst_r;
+    double umax, re;
+    int max_steps;
+    double tol;
+    double arrival;
+    int want_fields;       /* keep the final velocity field for lbgpu_server_result */
+} lbgpu_request;
+
+typedef struct {
+    double arrival, admit, finish;  /* seconds after the run's start */
+    long long steps, nodes;
+    int converged, done;            /* converged: 1 steady, 0 step cap, -1 diverged */
+    double last_change;             /* velocity change over the last check interval */
+} lbgpu_result;
+
+typedef struct lbgpu_server lbgpu_server;
+int lbgpu_server_create(int precision, size_t budget_bytes, int check_every, lbgpu_server **out);
+int lbgpu_server_destroy(lbgpu_server *s);
+int lbgpu_server_set_scheme(lbgpu_server *s, int size_class, int scheme);
+int lbgpu_server_set_shape(lbgpu_server *s, int size_class, int tile_width, int nodes_per_thread);
+int lbgpu_server_set_persistent(lbgpu_server *s, int persistent);
+int lbgpu_server_set_threads(lbgpu_server *s, int threads);
+int lbgpu_server_set_offset_scale(lbgpu_server *s, int scale_log2);
+int lbgpu_server_submit(lbgpu_server *s, const lbgpu_request *r, int *id);
+int lbgpu_server_run(lbgpu_server *s, int batched);
+int lbgpu_server_result(lbgpu_server *s, int id, lbgpu_result *out, double *ux, double *uy);
+/* out[0] makespan (s), out[1] lattice updates, out[2] peak resident requests, out[3] peak bytes */
+int lbgpu_server_stats(lbgpu_server *s, double out[4]);
+
+/* Autotuner for the scheme of batch members of one size: copies of a cylinder channel of
+ * lx x ly (enough for about 8M nodes, at most 64) step together in a batch, once in the pull
+ * and once in the AA scheme; returns the faster one (*scheme) and both timings of `steps`
+ * batch steps. */
 int lbgpu_tune_scheme(int precision, int lx, int ly, int steps, int *scheme, float *ms_pull,
                       float *ms_aa);
 void *lbgpu_stream(lbgpu_lattice *lat);           /* the lattice's cudaStream_t            */

@@ -1,11 +1,16 @@
 // batch.cu -- many independent lattices advanced together (lbgpu_batch_* of include/lbgpu.h).
 //
-// Every step of every member runs in one persistent launch per scheme: a grid of
-// (blocks per SM x SMs) blocks walks a work list of tiles (member, x0, y0, tile shape).  Steps
-// are grouped in chunks of 50 (an even count) captured once as a CUDA graph: the kernels read
-// each member's buffers and parities from a device descriptor array, so the same graph
-// replays chunk after chunk; it is re-captured only when the membership changes.  Tile shapes
-// are chosen per size class of member (node count), by hand or by lbgpu_batch_autotune.
+// Every step of every member runs in at most four launches, one per kind of step: the pull step
+// of the two-buffer members (one node per thread, or for 16-bit storage optionally four nodes
+// per thread), and the even and the odd AA step of the in-place members (AA members are kept in
+// two lists by the parity of their phase, so each list runs one kind at a time).  A launch walks a work list of tiles (member, x0, y0, tile width) of 128, 256 or 512
+// nodes, one per thread: either a persistent grid of (blocks per SM x SMs) blocks strides
+// through it, or one block per tile.
+// Steps are grouped in chunks of 50 (an even count) captured once as a CUDA graph: the kernels
+// read each member's buffers and parities from a device descriptor array, so the same graph
+// replays chunk after chunk; it is re-captured when the membership or the launch form changes.
+// Tile widths are chosen per size class of member (node count), the threads per tile and the
+// launch form per batch, by hand or by lbgpu_batch_autotune.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -21,6 +26,8 @@ namespace {
 
 constexpr int kClasses = 6;     // node-count classes: < 16K, 64K, 256K, 1M, 4M, above
 constexpr int kChunk = 50;      // steps per captured graph (even: buffer parities repeat)
+constexpr int kLists = 4;       // pull, pull four nodes a thread; AA of phase parity 0, 1 at rebuild
+constexpr int kQuad = 3;        // shape of the four-nodes-a-thread pull tiles (16-bit storage)
 
 int size_class(long long nodes)
 {
@@ -29,9 +36,9 @@ int size_class(long long nodes)
     return c;
 }
 
-// Tiles of width 32 << (shape & 3) and (128 / width) << (shape >> 2) rows.
-int tile_w(int shape) { return 32 << (shape & 3); }
-int tile_h(int shape) { return (lbgpu::BATCH_THREADS / tile_w(shape)) << (shape >> 2); }
+// Tiles of width 32 << shape and threads / width rows; quad tiles 128 wide, threads / 32 rows.
+int tile_w(int shape) { return shape == kQuad ? 128 : 32 << shape; }
+int tile_h(int shape, int threads) { return shape == kQuad ? threads / 32 : threads / tile_w(shape); }
 
 }  // namespace
 
@@ -39,22 +46,21 @@ struct lbgpu_batch {
     int precision = 0;
     cudaStream_t stream = nullptr;
     std::vector<lbgpu_lattice *> members;   // slot -> lattice (null: free slot)
-    int shape[kClasses] = {2, 2, 2, 2, 2, 2};  // 128 wide, one row per thread
+    int shape[kClasses] = {2, 2, 2, 2, 2, 2};  // 0..2: 32 << shape wide; kQuad: 16-bit quad pull
+    int threads = 128;                       // nodes per tile = threads per block
+    bool persistent = true;
     BatchInst *d_inst = nullptr;
     int cap_inst = 0;
-    BatchWork *d_work[2] = {nullptr, nullptr};
-    int cap_work[2] = {0, 0};
-    int *d_nwork = nullptr;                  // [2]
-    int nwork[2] = {0, 0};
-    int grid[2] = {0, 0};
+    BatchWork *d_work[kLists] = {nullptr, nullptr, nullptr, nullptr};
+    int cap_work[kLists] = {0, 0, 0, 0};
+    int nwork[kLists] = {0, 0, 0, 0};
+    int per_sm[4][3] = {};                   // resident blocks per SM, [kind][threads 128/256/512]
+    int sms = 0;
+    int aa_phase = 0;                        // phase parity of list 2 now (list 3: the other)
     std::vector<BatchInst> h_inst;
     bool dirty = true;                       // descriptors or work lists must be rebuilt
     cudaEvent_t order = nullptr;             // orders the batch stream against members' streams
-    cudaGraphExec_t graph = nullptr;
-    int graph_grid[2] = {0, 0};               // values the captured graph has baked in
-    BatchWork *graph_work[2] = {nullptr, nullptr};
-    BatchInst *graph_inst = nullptr;
-    bool graph_has[2] = {false, false};
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};   // one chunk, by aa_phase
     int launches = 0;
 };
 
@@ -106,60 +112,61 @@ void advance(Lattice &L, int m)
     }
 }
 
-int ensure_capacity(lbgpu_batch *b, int ninst, int nw0, int nw1)
+int ensure_capacity(lbgpu_batch *b, int ninst, const int *need)
 {
     if (ninst > b->cap_inst) {
         if (b->d_inst) cudaFree(b->d_inst);
+        b->d_inst = nullptr;
         b->cap_inst = std::max(ninst, 2 * b->cap_inst);
         void *p = nullptr;
         if (int rc = batch_error(cudaMalloc(&p, (size_t)b->cap_inst * sizeof(BatchInst)), "cudaMalloc(batch members)")) return rc;
         b->d_inst = static_cast<BatchInst *>(p);
     }
-    const int need[2] = {nw0, nw1};
-    for (int s = 0; s < 2; ++s)
+    for (int s = 0; s < kLists; ++s)
         if (need[s] > b->cap_work[s]) {
             if (b->d_work[s]) cudaFree(b->d_work[s]);
+            b->d_work[s] = nullptr;
             b->cap_work[s] = std::max(need[s], 2 * b->cap_work[s]);
             void *p = nullptr;
             if (int rc = batch_error(cudaMalloc(&p, (size_t)b->cap_work[s] * sizeof(BatchWork)), "cudaMalloc(batch tiles)")) return rc;
             b->d_work[s] = static_cast<BatchWork *>(p);
         }
-    if (!b->d_nwork) {
-        void *p = nullptr;
-        if (int rc = batch_error(cudaMalloc(&p, 2 * sizeof(int)), "cudaMalloc(batch counts)")) return rc;
-        b->d_nwork = static_cast<int *>(p);
-    }
     return LB_OK;
 }
 
-void drop_graph(lbgpu_batch *b)
+void drop_graphs(lbgpu_batch *b)
 {
-    if (b->graph) {
-        cudaGraphExecDestroy(b->graph);
-        b->graph = nullptr;
-    }
+    for (cudaGraphExec_t &g : b->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
 }
 
 // Rebuild descriptors and work lists from the members' current states.
 int rebuild(lbgpu_batch *b)
 {
-    std::vector<BatchWork> work[2];
+    std::vector<BatchWork> work[kLists];
     b->h_inst.assign(b->members.size(), BatchInst{});
     for (size_t i = 0; i < b->members.size(); ++i) {
         lbgpu_lattice *m = b->members[i];
         if (!m) continue;
         const Lattice &L = m->L;
         b->h_inst[i] = describe(L);
-        const int sh = b->shape[size_class((long long)L.lx * L.ly)];
-        const int tw = tile_w(sh), th = tile_h(sh);
-        const int s = (L.scheme == LBGPU_AA) ? 1 : 0;
+        int sh = b->shape[size_class((long long)L.lx * L.ly)];
+        if (sh == kQuad && L.scheme == LBGPU_AA) sh = 2;   // AA steps run one node per thread
+        const int tw = tile_w(sh), th = tile_h(sh, b->threads);
+        const int s = (L.scheme == LBGPU_AA) ? 2 + b->h_inst[i].phase0 : (sh == kQuad ? 1 : 0);
         for (int y0 = 1; y0 <= L.ly; y0 += th)
             for (int x0 = 1; x0 <= L.lx; x0 += tw) work[s].push_back(BatchWork{(int)i, x0, y0, sh});
     }
-    if (int rc = ensure_capacity(b, (int)std::max<size_t>(b->h_inst.size(), 1), (int)work[0].size(), (int)work[1].size())) return rc;
-    for (int s = 0; s < 2; ++s) {
-        b->nwork[s] = (int)work[s].size();
-        if (b->nwork[s])
+    b->aa_phase = 0;
+    int need[kLists];
+    for (int s = 0; s < kLists; ++s) need[s] = (int)work[s].size();
+    if (int rc = ensure_capacity(b, (int)std::max<size_t>(b->h_inst.size(), 1), need)) return rc;
+    for (int s = 0; s < kLists; ++s) {
+        b->nwork[s] = need[s];
+        if (need[s])
             if (int rc = batch_error(cudaMemcpyAsync(b->d_work[s], work[s].data(), work[s].size() * sizeof(BatchWork),
                                                      cudaMemcpyHostToDevice, b->stream), "upload batch tiles"))
                 return rc;
@@ -168,35 +175,44 @@ int rebuild(lbgpu_batch *b)
         if (int rc = batch_error(cudaMemcpyAsync(b->d_inst, b->h_inst.data(), b->h_inst.size() * sizeof(BatchInst),
                                                  cudaMemcpyHostToDevice, b->stream), "upload batch members"))
             return rc;
-    if (int rc = batch_error(cudaMemcpyAsync(b->d_nwork, b->nwork, 2 * sizeof(int), cudaMemcpyHostToDevice, b->stream),
-                             "upload batch counts"))
-        return rc;
     // the host arrays are read asynchronously: keep them alive until the copies finish
     if (int rc = batch_error(cudaStreamSynchronize(b->stream), "batch rebuild")) return rc;
-    int sms = 0, dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    for (int s = 0; s < 2; ++s) {
-        const int per_sm = std::max(1, lbgpu::batch_blocks_per_sm(b->precision, s == 1 ? LBGPU_AA : LBGPU_PULL));
-        b->grid[s] = per_sm * sms;   // fixed: surplus blocks find no tile and exit
+    if (!b->sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+        for (int kind = 0; kind < 4; ++kind)
+            for (int t = 0; t < 3; ++t)
+                b->per_sm[kind][t] = std::max(1, lbgpu::batch_blocks_per_sm(b->precision, kind, 128 << t));
     }
-    if (b->grid[0] != b->graph_grid[0] || b->grid[1] != b->graph_grid[1] ||
-        b->d_work[0] != b->graph_work[0] || b->d_work[1] != b->graph_work[1] || b->d_inst != b->graph_inst ||
-        (b->nwork[0] > 0) != b->graph_has[0] || (b->nwork[1] > 0) != b->graph_has[1])
-        drop_graph(b);
+    drop_graphs(b);
     b->dirty = false;
     return LB_OK;
 }
 
-// k-th step of a chunk for both schemes.
+// k-th step of a chunk: one launch per non-empty work list.
 void launch_step(lbgpu_batch *b, int k)
 {
-    for (int s = 0; s < 2; ++s)
-        if (b->nwork[s]) {
-            lbgpu::launch_batch(b->precision, s == 1 ? LBGPU_AA : LBGPU_PULL, b->d_inst, b->d_work[s],
-                                b->d_nwork + s, b->grid[s], k, b->stream);
-            ++b->launches;
+    for (int s = 0; s < kLists; ++s) {
+        if (!b->nwork[s]) continue;
+        int kind = s == 0 ? lbgpu::BATCH_PULL : lbgpu::BATCH_PULL4;
+        if (s >= 2) {
+            const int phase = (s == 2) ? b->aa_phase : 1 - b->aa_phase;
+            kind = ((phase + k) & 1) ? lbgpu::BATCH_AA_ODD : lbgpu::BATCH_AA_EVEN;
         }
+        const int t = b->threads == 512 ? 2 : (b->threads == 256 ? 1 : 0);
+        const int grid = b->persistent ? std::min(b->per_sm[kind][t] * b->sms, b->nwork[s]) : b->nwork[s];
+        lbgpu::launch_batch(b->precision, kind, b->threads, b->persistent, b->d_inst, b->d_work[s], b->nwork[s],
+                            grid, k, b->stream);
+        ++b->launches;
+    }
+}
+
+int launches_per_step(const lbgpu_batch *b)
+{
+    int n = 0;
+    for (int s = 0; s < kLists; ++s) n += b->nwork[s] ? 1 : 0;
+    return n;
 }
 
 int capture_chunk(lbgpu_batch *b)
@@ -208,15 +224,9 @@ int capture_chunk(lbgpu_batch *b)
     b->launches = before;
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (e != cudaSuccess) return batch_error(e, "end capture");
-    e = cudaGraphInstantiate(&b->graph, g, 0);
+    e = cudaGraphInstantiate(&b->graph[b->aa_phase], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return batch_error(e, "graph instantiate");
-    for (int s = 0; s < 2; ++s) {
-        b->graph_grid[s] = b->grid[s];
-        b->graph_work[s] = b->d_work[s];
-        b->graph_has[s] = b->nwork[s] > 0;
-    }
-    b->graph_inst = b->d_inst;
     return LB_OK;
 }
 
@@ -260,6 +270,8 @@ int lbgpu_batch_create(int precision, lbgpu_batch **out)
         return set_error(LB_ERR_ARG, "lbgpu_batch_create: precision %d", precision);
     lbgpu_batch *b = new lbgpu_batch;
     b->precision = precision;
+    if (precision == LBGPU_F16 || precision == LBGPU_BF16)
+        for (int c = 2; c < kClasses; ++c) b->shape[c] = kQuad;   // lattices of 64K nodes and more
     if (int rc = batch_error(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "batch stream")) {
         delete b;
         return rc;
@@ -277,10 +289,9 @@ int lbgpu_batch_destroy(lbgpu_batch *b)
 {
     if (!b) return LB_OK;
     cudaStreamSynchronize(b->stream);
-    drop_graph(b);
+    drop_graphs(b);
     if (b->d_inst) cudaFree(b->d_inst);
-    for (int s = 0; s < 2; ++s) if (b->d_work[s]) cudaFree(b->d_work[s]);
-    if (b->d_nwork) cudaFree(b->d_nwork);
+    for (int s = 0; s < kLists; ++s) if (b->d_work[s]) cudaFree(b->d_work[s]);
     cudaEventDestroy(b->order);
     cudaStreamDestroy(b->stream);
     delete b;
@@ -327,29 +338,54 @@ int lbgpu_batch_size(lbgpu_batch *b)
     return n;
 }
 
-int lbgpu_batch_set_shape(lbgpu_batch *b, int size_class_, int tile_width, int rows_per_thread)
+int lbgpu_batch_set_shape(lbgpu_batch *b, int size_class_, int tile_width, int nodes_per_thread)
 {
     if (!b || size_class_ < 0 || size_class_ >= kClasses)
         return set_error(LB_ERR_ARG, "lbgpu_batch_set_shape: size class %d", size_class_);
-    int ws = -1, rs = -1;
+    int ws = -1;
     for (int k = 0; k < 3; ++k) if ((32 << k) == tile_width) ws = k;
-    for (int k = 0; k < 3; ++k) if ((1 << k) == rows_per_thread) rs = k;
-    if (ws < 0 || rs < 0)
-        return set_error(LB_ERR_ARG, "lbgpu_batch_set_shape: tile width %d (32, 64, 128), rows %d (1, 2, 4)",
-                         tile_width, rows_per_thread);
-    b->shape[size_class_] = ws | (rs << 2);
+    const bool quad_ok = (b->precision == LBGPU_F16 || b->precision == LBGPU_BF16) && tile_width == 128;
+    if (ws < 0 || (nodes_per_thread != 1 && !(nodes_per_thread == 4 && quad_ok)))
+        return set_error(LB_ERR_ARG, "lbgpu_batch_set_shape: tile width %d (32, 64, 128), nodes per thread %d "
+                         "(1; 4 with width 128 and 16-bit storage)", tile_width, nodes_per_thread);
+    b->shape[size_class_] = nodes_per_thread == 4 ? kQuad : ws;
     b->dirty = true;
     return LB_OK;
 }
 
-int lbgpu_batch_get_shape(lbgpu_batch *b, int size_class_, int *tile_width, int *rows_per_thread)
+int lbgpu_batch_get_shape(lbgpu_batch *b, int size_class_, int *tile_width, int *nodes_per_thread)
 {
     if (!b || size_class_ < 0 || size_class_ >= kClasses)
         return set_error(LB_ERR_ARG, "lbgpu_batch_get_shape: size class %d", size_class_);
     if (tile_width) *tile_width = tile_w(b->shape[size_class_]);
-    if (rows_per_thread) *rows_per_thread = 1 << (b->shape[size_class_] >> 2);
+    if (nodes_per_thread) *nodes_per_thread = b->shape[size_class_] == kQuad ? 4 : 1;
     return LB_OK;
 }
+
+int lbgpu_batch_set_persistent(lbgpu_batch *b, int persistent)
+{
+    if (!b) return set_error(LB_ERR_ARG, "lbgpu_batch_set_persistent: null batch");
+    if (b->persistent != (persistent != 0)) {
+        b->persistent = persistent != 0;
+        drop_graphs(b);
+    }
+    return LB_OK;
+}
+
+int lbgpu_batch_get_persistent(lbgpu_batch *b) { return b && b->persistent ? 1 : 0; }
+
+int lbgpu_batch_set_threads(lbgpu_batch *b, int threads)
+{
+    if (!b || (threads != 128 && threads != 256 && threads != 512))
+        return set_error(LB_ERR_ARG, "lbgpu_batch_set_threads: %d threads per tile (128, 256, 512)", threads);
+    if (b->threads != threads) {
+        b->threads = threads;
+        b->dirty = true;
+    }
+    return LB_OK;
+}
+
+int lbgpu_batch_get_threads(lbgpu_batch *b) { return b ? b->threads : 0; }
 
 int lbgpu_batch_size_class(long long nodes) { return size_class(nodes); }
 
@@ -380,10 +416,10 @@ int lbgpu_batch_step(lbgpu_batch *b, int nsteps)
     if (int rc = order_before(b)) return rc;
     int done = 0;
     while (nsteps - done >= kChunk) {
-        if (!b->graph)
+        if (!b->graph[b->aa_phase])
             if (int rc = capture_chunk(b)) return rc;
-        if (int rc = batch_error(cudaGraphLaunch(b->graph, b->stream), "graph launch")) return rc;
-        b->launches += kChunk * ((b->nwork[0] ? 1 : 0) + (b->nwork[1] ? 1 : 0));
+        if (int rc = batch_error(cudaGraphLaunch(b->graph[b->aa_phase], b->stream), "graph launch")) return rc;
+        b->launches += kChunk * launches_per_step(b);
         done += kChunk;
     }
     const int rem = nsteps - done;
@@ -393,7 +429,9 @@ int lbgpu_batch_step(lbgpu_batch *b, int nsteps)
         if (m) advance(m->L, nsteps);
     if (int rc = order_after(b)) return rc;
     if (rem & 1) {
-        // parities changed: new descriptors before the next call (a chunk's graph reads them)
+        // parities changed: new descriptors before the next call (a chunk's graph reads them),
+        // and the AA lists swap their kind of step
+        b->aa_phase ^= 1;
         for (size_t i = 0; i < b->members.size(); ++i)
             if (b->members[i]) b->h_inst[i] = describe(b->members[i]->L);
         if (int rc = batch_error(cudaMemcpyAsync(b->d_inst, b->h_inst.data(), b->h_inst.size() * sizeof(BatchInst),
@@ -430,26 +468,51 @@ int lbgpu_batch_synchronize(lbgpu_batch *b)
 
 int lbgpu_batch_last_launches(lbgpu_batch *b) { return b ? b->launches : 0; }
 
-// For every size class present, time `steps` batch steps with each tile shape and keep the
-// fastest.  The members really step (3 x 3 shapes x `steps` steps per class).
+// One candidate setting: an untimed batch step first (work-list rebuild, first-step path), so
+// that the timed steps hold only the launches the setting makes.
+static int time_setting(lbgpu_batch *b, int steps, float *ms)
+{
+    if (int rc = lbgpu_batch_step(b, 1)) return rc;
+    return lbgpu_batch_step_timed(b, steps, ms);
+}
+
+// Threads per tile and launch form first (six combinations, shapes as set), then for every size
+// class present the three tile widths (and for 16-bit storage the four-nodes-a-thread pull),
+// each timed over `steps` batch steps after one untimed step; the fastest is kept at each
+// stage.  The members really step (6 x (steps + 1), then 3 or 4 x (steps + 1) per class).
 int lbgpu_batch_autotune(lbgpu_batch *b, int steps, float *best_ms_out)
 {
     if (!b || steps < 1) return set_error(LB_ERR_ARG, "lbgpu_batch_autotune: bad arguments");
     bool present[kClasses] = {false};
     for (lbgpu_lattice *m : b->members)
         if (m) present[size_class((long long)m->L.lx * m->L.ly)] = true;
+    {
+        float best = 1e30f;
+        int best_t = b->threads, best_p = b->persistent ? 1 : 0;
+        for (int t = 128; t <= 512; t *= 2)
+            for (int p = 0; p < 2; ++p) {
+                lbgpu_batch_set_threads(b, t);
+                lbgpu_batch_set_persistent(b, p);
+                float ms = 0.f;
+                if (int rc = time_setting(b, steps, &ms)) return rc;
+                if (ms < best) { best = ms; best_t = t; best_p = p; }
+            }
+        lbgpu_batch_set_threads(b, best_t);
+        lbgpu_batch_set_persistent(b, best_p);
+    }
     for (int c = 0; c < kClasses; ++c) {
+        if (best_ms_out) best_ms_out[c] = 0.f;
         if (!present[c]) continue;
         float best = 1e30f;
         int best_shape = b->shape[c];
-        for (int ws = 0; ws < 3; ++ws)
-            for (int rs = 0; rs < 3; ++rs) {
-                b->shape[c] = ws | (rs << 2);
-                b->dirty = true;
-                float ms = 0.f;
-                if (int rc = lbgpu_batch_step_timed(b, steps, &ms)) return rc;
-                if (ms < best) { best = ms; best_shape = b->shape[c]; }
-            }
+        const int nshapes = (b->precision == LBGPU_F16 || b->precision == LBGPU_BF16) ? 4 : 3;
+        for (int ws = 0; ws < nshapes; ++ws) {
+            b->shape[c] = ws;
+            b->dirty = true;
+            float ms = 0.f;
+            if (int rc = time_setting(b, steps, &ms)) return rc;
+            if (ms < best) { best = ms; best_shape = ws; }
+        }
         b->shape[c] = best_shape;
         b->dirty = true;
         if (best_ms_out) best_ms_out[c] = best;
@@ -458,18 +521,31 @@ int lbgpu_batch_autotune(lbgpu_batch *b, int steps, float *best_ms_out)
 }
 
 // Choose between the two-buffer pull scheme and the in-place AA scheme for lattices of one
-// size: time `steps` steps of a cylinder channel of that size in each scheme on their own.
+// size as batch members: for each scheme, copies of a cylinder channel of that size (enough for
+// about 8M nodes, at most 64) step together in a batch, and `steps` batch steps are timed.
 int lbgpu_tune_scheme(int precision, int lx, int ly, int steps, int *scheme, float *ms_pull, float *ms_aa)
 {
+    if (lx < 4 || ly < 4 || steps < 1) return set_error(LB_ERR_ARG, "lbgpu_tune_scheme: bad arguments");
+    const long long nodes = (long long)lx * ly;
+    const int copies = (int)std::max(1LL, std::min(64LL, (8LL << 20) / nodes));
     float t[2] = {0.f, 0.f};
     for (int s = 0; s < 2; ++s) {
-        lbgpu_lattice *h = nullptr;
-        if (int rc = lbgpu_create(lx, ly, precision, s == 0 ? LBGPU_PULL : LBGPU_AA, &h)) return rc;
-        int rc = lbgpu_setup_cylinder(h, lx / 5 + 1, ly / 2 + 1, ly / 10 + 1, 0.02, 100.0,
+        std::vector<lbgpu_lattice *> lats;
+        lbgpu_batch *b = nullptr;
+        int rc = lbgpu_batch_create(precision, &b);
+        for (int c = 0; c < copies && rc == LB_OK; ++c) {
+            lbgpu_lattice *h = nullptr;
+            rc = lbgpu_create(lx, ly, precision, s == 0 ? LBGPU_PULL : LBGPU_AA, &h);
+            if (rc) break;
+            lats.push_back(h);
+            rc = lbgpu_setup_cylinder(h, lx / 5 + 1, ly / 2 + 1, ly / 10 + 1, 0.02, 100.0,
                                       LBGPU_WALL_BOUNCEBACK, LBGPU_OUTLET_CONST, nullptr);
-        if (rc == LB_OK) rc = lbgpu_step(h, 2);
-        if (rc == LB_OK) rc = lbgpu_step_timed(h, steps, &t[s]);
-        lbgpu_destroy(h);
+            if (rc == LB_OK) rc = lbgpu_batch_add(b, h, nullptr);
+        }
+        if (rc == LB_OK) rc = lbgpu_batch_step(b, 2);
+        if (rc == LB_OK) rc = lbgpu_batch_step_timed(b, steps, &t[s]);
+        if (b) lbgpu_batch_destroy(b);
+        for (lbgpu_lattice *h : lats) lbgpu_destroy(h);
         if (rc) return rc;
     }
     if (ms_pull) *ms_pull = t[0];

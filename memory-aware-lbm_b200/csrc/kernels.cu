@@ -299,11 +299,17 @@ __device__ __forceinline__ void pull_node(const Geo &g, const S *__restrict__ sr
     typename Work<S>::W f[9];
     const bool edge = g.perimeter(X, Y);
     const int p = edge ? g.pidx(X, Y) : 0;
+    if (!edge) {
 #pragma unroll
-    for (int i = 0; i < 9; ++i) {
-        const int sx = X - cx(i), sy = Y - cy(i);
-        f[i] = Work<S>::load(g.interior(sx, sy) ? plane(src, g, i)[g.idx(sx, sy)]
-                                                : side[(size_t)i * g.nper + p], i, inv);
+        for (int i = 0; i < 9; ++i)
+            f[i] = Work<S>::load(plane(src, g, i)[o - cx(i) - (long long)cy(i) * g.pitch], i, inv);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const int sx = X - cx(i), sy = Y - cy(i);
+            f[i] = Work<S>::load(g.interior(sx, sy) ? plane(src, g, i)[g.idx(sx, sy)]
+                                                    : side[(size_t)i * g.nper + p], i, inv);
+        }
     }
     collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
 #pragma unroll
@@ -315,17 +321,16 @@ __device__ __forceinline__ void pull_node(const Geo &g, const S *__restrict__ sr
     }
 }
 
+//
+// pull_quad runs the four nodes x0..x0+3 of row Y (x0 = 1 mod 4) for one lane of a warp whose
+// lanes cover 128 consecutive nodes; the whole warp must call it together (shuffles).
 template <class S>
-__global__ void __launch_bounds__(BX) k_pull4h(Geo g, const S *__restrict__ src, S *__restrict__ dst,
-                                               const uint8_t *__restrict__ tag,
-                                               const double *__restrict__ bc, double omega,
-                                               S *__restrict__ side, float sc, float inv)
+__device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ src, S *__restrict__ dst,
+                                          const uint8_t *__restrict__ tag, const double *__restrict__ bc,
+                                          double omega, S *__restrict__ side, float sc, float inv, int x0,
+                                          int Y, int lane)
 {
     using H = Half2Ops<S>;
-    const int t = blockIdx.x * BX + threadIdx.x;
-    const int x0 = 1 + 4 * t;
-    const int Y = blockIdx.y + 1;
-    const int lane = threadIdx.x & 31;
     const int xw0 = x0 - 4 * lane;
     const bool vec = (xw0 >= 2) && (xw0 + 127 <= g.lx - 1) && (Y >= 2) && (Y <= g.ly - 1);
     if (!vec) {
@@ -378,6 +383,16 @@ __global__ void __launch_bounds__(BX) k_pull4h(Geo g, const S *__restrict__ src,
         w.y = H::pack(D[2][i], D[3][i]);
         *reinterpret_cast<uint2 *>(plane(dst, g, i) + o) = w;
     }
+}
+
+template <class S>
+__global__ void __launch_bounds__(BX) k_pull4h(Geo g, const S *__restrict__ src, S *__restrict__ dst,
+                                               const uint8_t *__restrict__ tag,
+                                               const double *__restrict__ bc, double omega,
+                                               S *__restrict__ side, float sc, float inv)
+{
+    const int t = blockIdx.x * BX + threadIdx.x;
+    pull_quad<S>(g, src, dst, tag, bc, omega, side, sc, inv, 1 + 4 * t, blockIdx.y + 1, threadIdx.x & 31);
 }
 
 // Propagation of C_n in `src` into `dst` (form C -> form L), ghost ring included; stale
@@ -489,47 +504,79 @@ __global__ void __launch_bounds__(BX) k_aa_odd(Geo g, S *__restrict__ a,
 
 // ---- many lattices in one launch ----------------------------------------------------------
 //
-// One time step of every lattice of a batch: a fixed grid of blocks walks a work list of tiles
-// (lattice, x0, y0, shape).  A tile is `tw` = 32 << (shape & 3) nodes wide and (128 / tw) << r
-// rows high (r = shape >> 2), one block of 128 threads, each thread doing 1 << r nodes down y.
-// A lattice's buffers and parities at step k of a chunk follow from its state at the chunk's
-// start (BatchInst), so a CUDA graph of the chunk's launches replays unchanged.  Each node runs
-// the same function as the single-lattice kernels, so a lattice's result is the same in the
-// batch and alone.
-template <class S, bool AA>
-__global__ void __launch_bounds__(BATCH_THREADS) k_batch(const BatchInst *__restrict__ insts,
-                                                         const BatchWork *__restrict__ work,
-                                                         const int *__restrict__ nwork_p, int k)
+// One time step of every lattice of a batch: one launch per kind of step (pull, AA even, AA
+// odd) over a work list of tiles (lattice, x0, y0, tile width).  A tile is BT nodes, one per
+// thread of a BT-thread block (BT = 128, 256 or 512): 32 << shape nodes wide and BT / width
+// rows high.  The launch is either persistent (a grid of blocks-per-SM x SMs blocks strides
+// through the list) or one block per tile.  A lattice's buffers and parities at step k of a
+// chunk follow from its state at the chunk's start (BatchInst), so a CUDA graph of the chunk's
+// launches replays unchanged.  Each node runs the same function as the single-lattice kernels,
+// so a lattice's result is the same in the batch and alone.
+//
+// One node per thread is deliberate: a loop over several nodes per thread lets the compiler keep
+// the nine source and nine destination plane addresses live across iterations, which doubled the
+// registers per thread (and halved the resident warps) of the loop form.  Larger tiles instead
+// spread the two dependent descriptor loads at the start of a tile over more nodes.  The kernel
+// is bound by memory latency at the occupancy its registers allow (ncu: 62 % of warps active
+// at 40 registers against 86 % for the single-lattice pull kernel at 32), so the minimum blocks
+// per SM below cap the registers as far as that costs no (or a few bytes of) spills: 2048
+// threads a SM leave 32 registers a thread, 1280 leave 48, 1024 leave 64, 768 leave 80.
+template <class S, int KIND, bool PERSIST, int BT>
+constexpr int batch_min_blocks()
 {
-    const int nwork = *nwork_p;
-    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-        const BatchWork it = work[w];
-        const BatchInst &d = insts[it.inst];
-        const Geo g = d.g;
-        const int tw = 32 << (it.shape & 3);
-        const int r = it.shape >> 2;
-        const int dx = threadIdx.x & (tw - 1);
-        const int rows = 1 << r;
-        const int dy0 = (threadIdx.x / tw) << r;
-        const int X = it.x0 + dx;
-        if (X > g.lx) continue;
-        const int tau = d.tau0 + k;
-        S *side = static_cast<S *>(d.side) + (size_t)(tau & 1) * 9 * (size_t)g.nper;
-        for (int j = 0; j < rows; ++j) {
-            const int Y = it.y0 + dy0 + j;
-            if (Y > g.ly) break;
-            if (!AA) {
-                const int src = d.cur0 ^ (k & 1);
-                pull_node<S>(g, static_cast<const S *>(d.buf[src]), static_cast<S *>(d.buf[src ^ 1]),
-                             d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, X, Y);
-            } else if (((d.phase0 + k) & 1) == 0) {
-                aa_even_node<S>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, d.omega, side,
-                                d.scale, d.inv_scale, X, Y);
-            } else {
-                aa_odd_node<S>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, d.omega, side,
-                               d.scale, d.inv_scale, X, Y);
-            }
+    int b128 = 0;   // blocks of 128 threads
+    if (sizeof(S) == 8) b128 = KIND == BATCH_PULL ? (PERSIST ? 6 : 10) : (KIND == BATCH_AA_EVEN ? 6 : 5);
+    else if (KIND == BATCH_PULL) b128 = PERSIST ? 8 : 16;
+    else if (KIND == BATCH_AA_EVEN) b128 = PERSIST ? 8 : 10;
+    else if (KIND == BATCH_PULL4) b128 = 6;
+    else b128 = (sizeof(S) == 4 && !PERSIST) ? 6 : 8;
+    return b128 * 128 / BT > 0 ? b128 * 128 / BT : 1;
+}
+
+template <class S, int KIND, int BT>
+__device__ __forceinline__ void batch_node(const BatchInst *__restrict__ insts, const BatchWork it, int k)
+{
+    const BatchInst &d = insts[it.inst];
+    const Geo g = d.g;
+    if constexpr (KIND == BATCH_PULL4) {
+        if constexpr (sizeof(S) == 2) {
+            // warp w of the block: row y0 + w, lanes x0 + 4 lane .. x0 + 4 lane + 3
+            const int Y = it.y0 + (int)(threadIdx.x >> 5);
+            if (Y > g.ly) return;                       // uniform over the warp
+            const int lane = threadIdx.x & 31;
+            S *side = static_cast<S *>(d.side) + (size_t)((d.tau0 + k) & 1) * 9 * (size_t)g.nper;
+            const int src = d.cur0 ^ (k & 1);
+            pull_quad<S>(g, static_cast<const S *>(d.buf[src]), static_cast<S *>(d.buf[src ^ 1]), d.tag,
+                         d.bc, d.omega, side, d.scale, d.inv_scale, it.x0 + 4 * lane, Y, lane);
         }
+        return;
+    }
+    const int lw = 5 + it.shape;                       // log2 of the tile width
+    const int X = it.x0 + (int)(threadIdx.x & ((1u << lw) - 1));
+    const int Y = it.y0 + (int)(threadIdx.x >> lw);
+    if (X > g.lx || Y > g.ly) return;
+    S *side = static_cast<S *>(d.side) + (size_t)((d.tau0 + k) & 1) * 9 * (size_t)g.nper;
+    if (KIND == BATCH_PULL) {
+        const int src = d.cur0 ^ (k & 1);
+        pull_node<S>(g, static_cast<const S *>(d.buf[src]), static_cast<S *>(d.buf[src ^ 1]), d.tag,
+                     d.bc, d.omega, side, d.scale, d.inv_scale, X, Y);
+    } else if (KIND == BATCH_AA_EVEN) {
+        aa_even_node<S>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, d.omega, side, d.scale,
+                        d.inv_scale, X, Y);
+    } else {
+        aa_odd_node<S>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, d.omega, side, d.scale,
+                       d.inv_scale, X, Y);
+    }
+}
+
+template <class S, int KIND, bool PERSIST, int BT>
+__global__ void __launch_bounds__(BT, (batch_min_blocks<S, KIND, PERSIST, BT>()))
+    k_batch(const BatchInst *__restrict__ insts, const BatchWork *__restrict__ work, int nwork, int k)
+{
+    if (PERSIST) {
+        for (int w = blockIdx.x; w < nwork; w += gridDim.x) batch_node<S, KIND, BT>(insts, work[w], k);
+    } else if ((int)blockIdx.x < nwork) {
+        batch_node<S, KIND, BT>(insts, work[blockIdx.x], k);
     }
 }
 
@@ -690,6 +737,29 @@ __global__ void __launch_bounds__(BX) k_init_cylinder(Geo g, S *__restrict__ buf
     }
 }
 
+// Tag plane of the cylinder channel, the same assignment order as the host builder
+// (dynamics_host.c lbgpu_build_cylinder, after unsteady.c:162-199): bulk or obstacle disk,
+// then the lower and upper wall rows, then the inlet and outlet columns of rows 2..ly-1.
+__global__ void __launch_bounds__(BX) k_cylinder_tags(Geo g, uint8_t *__restrict__ tag, int ox, int oy,
+                                                      int r, int lower, int upper)
+{
+    const int X = blockIdx.x * BX + threadIdx.x;
+    const int Y = blockIdx.y;
+    if (X > g.lx + 1) return;
+    int t = LBGPU_TAG_NONE;
+    if (g.interior(X, Y)) {
+        const long long dx = X - ox, dy = Y - oy;
+        t = dx * dx + dy * dy <= (long long)r * r ? LBGPU_TAG_BOUNCE_BACK : LBGPU_TAG_BGK;
+        if (Y == 1) t = lower;
+        if (Y == g.ly) t = upper;
+        if (Y >= 2 && Y <= g.ly - 1) {
+            if (X == 1) t = LBGPU_TAG_LEFT_REGULARIZED;
+            if (X == g.lx) t = LBGPU_TAG_RIGHT_PRESSURE_REGULARIZED;
+        }
+    }
+    tag[g.idx(X, Y)] = (uint8_t)t;
+}
+
 template <class S>
 __global__ void __launch_bounds__(BX) k_macros(Geo g, int view, const S *__restrict__ cur,
                                                const S *__restrict__ other,
@@ -820,6 +890,37 @@ __global__ void __launch_bounds__(BX) k_accumulate_velocity(Geo g, int view, con
     acc[n + k] += jy / rho;
 }
 
+// Steady-state residual: the largest |u - u_prev| over the interior (u_prev: the velocity at
+// the previous check, FP32 pairs, replaced by the current one).  *out holds the bits of a
+// non-negative float, so an integer atomicMax orders it; the caller clears it first.
+template <class S>
+__global__ void __launch_bounds__(BX) k_velocity_change(Geo g, int view, const S *__restrict__ cur,
+                                                        const S *__restrict__ other,
+                                                        const S *__restrict__ side,
+                                                        float2 *__restrict__ prev,
+                                                        unsigned *__restrict__ out, float inv)
+{
+    const int X = blockIdx.x * BX + threadIdx.x + 1;
+    const int Y = blockIdx.y + 1;
+    float d = 0.0f;
+    if (X <= g.lx) {
+        double f[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) f[i] = (double)logical(g, view, cur, other, side, X, Y, i, inv);
+        const double rho = ((f[0] + f[1]) + (f[2] + f[3])) + ((f[4] + f[5]) + (f[6] + f[7])) + f[8];
+        const float ux = (float)(((f[1] - f[3]) + (f[5] - f[6]) + (f[8] - f[7])) / rho);
+        const float uy = (float)(((f[2] - f[4]) + (f[5] - f[8]) + (f[6] - f[7])) / rho);
+        const size_t k = (size_t)(Y - 1) * g.lx + (X - 1);
+        const float2 p = prev[k];
+        d = sqrtf((ux - p.x) * (ux - p.x) + (uy - p.y) * (uy - p.y));
+        if (!(d == d)) d = 3.0e38f;   // a NaN counts as not converged
+        prev[k] = make_float2(ux, uy);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d = fmaxf(d, __shfl_xor_sync(0xffffffffu, d, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(d));
+}
+
 inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
 template <class S> S *B(const DevLattice &d, int b) { return static_cast<S *>(d.buf[b]); }
@@ -896,43 +997,71 @@ void launch_aa_odd(const DevLattice &d, int side_par, cudaStream_t s)
                        SIDE<S>(d, side_par), d.scale, d.inv_scale)));
 }
 
-template <class S>
-static void launch_batch_t(int scheme, const BatchInst *insts, const BatchWork *work, const int *nwork,
-                           int grid, int k, cudaStream_t s)
+template <class S, int KIND, int BT>
+static void launch_batch_b(bool persistent, const BatchInst *insts, const BatchWork *work, int nwork, int grid,
+                           int k, cudaStream_t s)
 {
-    if (scheme == LBGPU_AA) k_batch<S, true><<<grid, BATCH_THREADS, 0, s>>>(insts, work, nwork, k);
-    else k_batch<S, false><<<grid, BATCH_THREADS, 0, s>>>(insts, work, nwork, k);
+    if (persistent) k_batch<S, KIND, true, BT><<<grid, BT, 0, s>>>(insts, work, nwork, k);
+    else k_batch<S, KIND, false, BT><<<grid, BT, 0, s>>>(insts, work, nwork, k);
 }
 
-void launch_batch(int precision, int scheme, const BatchInst *insts, const BatchWork *work,
-                  const int *nwork, int grid, int k, cudaStream_t s)
+template <class S, int KIND>
+static void launch_batch_k(int bt, bool persistent, const BatchInst *insts, const BatchWork *work, int nwork,
+                           int grid, int k, cudaStream_t s)
+{
+    if (bt == 512) launch_batch_b<S, KIND, 512>(persistent, insts, work, nwork, grid, k, s);
+    else if (bt == 256) launch_batch_b<S, KIND, 256>(persistent, insts, work, nwork, grid, k, s);
+    else launch_batch_b<S, KIND, 128>(persistent, insts, work, nwork, grid, k, s);
+}
+
+template <class S>
+static void launch_batch_t(int kind, int bt, bool persistent, const BatchInst *insts, const BatchWork *work,
+                           int nwork, int grid, int k, cudaStream_t s)
+{
+    if (kind == BATCH_PULL) launch_batch_k<S, BATCH_PULL>(bt, persistent, insts, work, nwork, grid, k, s);
+    else if (kind == BATCH_AA_EVEN) launch_batch_k<S, BATCH_AA_EVEN>(bt, persistent, insts, work, nwork, grid, k, s);
+    else if (kind == BATCH_AA_ODD) launch_batch_k<S, BATCH_AA_ODD>(bt, persistent, insts, work, nwork, grid, k, s);
+    else if constexpr (sizeof(S) == 2) launch_batch_k<S, BATCH_PULL4>(bt, persistent, insts, work, nwork, grid, k, s);
+}
+
+void launch_batch(int precision, int kind, int threads, bool persistent, const BatchInst *insts,
+                  const BatchWork *work, int nwork, int grid, int k, cudaStream_t s)
 {
     switch (precision) {
-    case LBGPU_F64: launch_batch_t<double>(scheme, insts, work, nwork, grid, k, s); break;
-    case LBGPU_F32: launch_batch_t<float>(scheme, insts, work, nwork, grid, k, s); break;
-    case LBGPU_F16: launch_batch_t<__half>(scheme, insts, work, nwork, grid, k, s); break;
-    default: launch_batch_t<__nv_bfloat16>(scheme, insts, work, nwork, grid, k, s); break;
+    case LBGPU_F64: launch_batch_t<double>(kind, threads, persistent, insts, work, nwork, grid, k, s); break;
+    case LBGPU_F32: launch_batch_t<float>(kind, threads, persistent, insts, work, nwork, grid, k, s); break;
+    case LBGPU_F16: launch_batch_t<__half>(kind, threads, persistent, insts, work, nwork, grid, k, s); break;
+    default: launch_batch_t<__nv_bfloat16>(kind, threads, persistent, insts, work, nwork, grid, k, s); break;
     }
 }
 
-template <class S>
-static int blocks_t(int scheme)
+template <class S, int KIND>
+static int blocks_k(int bt)
 {
     int n = 0;
-    if (scheme == LBGPU_AA)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch<S, true>, BATCH_THREADS, 0);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch<S, false>, BATCH_THREADS, 0);
+    if (bt == 512) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch<S, KIND, true, 512>, 512, 0);
+    else if (bt == 256) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch<S, KIND, true, 256>, 256, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch<S, KIND, true, 128>, 128, 0);
     return n;
 }
 
-int batch_blocks_per_sm(int precision, int scheme)
+template <class S>
+static int blocks_t(int kind, int bt)
+{
+    if (kind == BATCH_PULL) return blocks_k<S, BATCH_PULL>(bt);
+    if (kind == BATCH_AA_EVEN) return blocks_k<S, BATCH_AA_EVEN>(bt);
+    if (kind == BATCH_AA_ODD) return blocks_k<S, BATCH_AA_ODD>(bt);
+    if constexpr (sizeof(S) == 2) return blocks_k<S, BATCH_PULL4>(bt);
+    return 0;
+}
+
+int batch_blocks_per_sm(int precision, int kind, int threads)
 {
     switch (precision) {
-    case LBGPU_F64: return blocks_t<double>(scheme);
-    case LBGPU_F32: return blocks_t<float>(scheme);
-    case LBGPU_F16: return blocks_t<__half>(scheme);
-    default: return blocks_t<__nv_bfloat16>(scheme);
+    case LBGPU_F64: return blocks_t<double>(kind, threads);
+    case LBGPU_F32: return blocks_t<float>(kind, threads);
+    case LBGPU_F16: return blocks_t<__half>(kind, threads);
+    default: return blocks_t<__nv_bfloat16>(kind, threads);
     }
 }
 
@@ -990,12 +1119,30 @@ void launch_init_cylinder(const DevLattice &d, int b, double umax, cudaStream_t 
     LBGPU_DISPATCH(d, (k_init_cylinder<S><<<grid, BX, 0, s>>>(d.g, B<S>(d, b), umax, d.scale)));
 }
 
+void launch_cylinder_tags(const DevLattice &d, int ox, int oy, int r, int wall_kind, cudaStream_t s)
+{
+    dim3 grid(cdiv(d.g.lx + 2, BX), d.g.ly + 2);
+    const bool bb = wall_kind == LBGPU_WALL_BOUNCEBACK;
+    k_cylinder_tags<<<grid, BX, 0, s>>>(d.g, const_cast<uint8_t *>(d.tag), ox, oy, r,
+                                        bb ? LBGPU_TAG_BOUNCE_BACK : LBGPU_TAG_LOWER_REGULARIZED,
+                                        bb ? LBGPU_TAG_BOUNCE_BACK : LBGPU_TAG_UPPER_REGULARIZED);
+}
+
 void launch_moments(const DevLattice &d, int view, int cur, int side_par, double *partial,
                     double *out, cudaStream_t s)
 {
     LBGPU_DISPATCH(d, (k_moments_rows<S><<<d.g.ly, RED_THREADS, 0, s>>>(d.g, view, B<S>(d, cur),
                        OTHER<S>(d, cur), SIDE<S>(d, side_par), d.tag, partial, d.inv_scale)));
     k_moments_final<<<1, RED_THREADS, 0, s>>>(d.g.ly, partial, out);
+}
+
+void launch_velocity_change(const DevLattice &d, int view, int cur, int side_par, void *prev,
+                            unsigned *out, cudaStream_t s)
+{
+    dim3 grid(cdiv(d.g.lx, BX), d.g.ly);
+    LBGPU_DISPATCH(d, (k_velocity_change<S><<<grid, BX, 0, s>>>(d.g, view, B<S>(d, cur),
+                       OTHER<S>(d, cur), SIDE<S>(d, side_par), static_cast<float2 *>(prev), out,
+                       d.inv_scale)));
 }
 
 void launch_accumulate_velocity(const DevLattice &d, int view, int cur, int side_par, double *acc,

@@ -41,6 +41,9 @@ void launch_upload(const DevLattice &d, int b, const double *in, int rec_stride,
 void launch_zgb_rho(const DevLattice &d, int view, int cur, int side_par, cudaStream_t s);
 void launch_zgb_apply(const DevLattice &d, cudaStream_t s);
 void launch_periodic(const DevLattice &d, int b, cudaStream_t s);
+// Tag plane of the cylinder channel (obstacle disk, walls of wall_kind, regularized inlet,
+// pressure-regularized outlet) written on the device.
+void launch_cylinder_tags(const DevLattice &d, int ox, int oy, int r, int wall_kind, cudaStream_t s);
 void launch_init_cylinder(const DevLattice &d, int b, double umax, cudaStream_t s);
 void launch_macros(const DevLattice &d, int view, int cur, int side_par, double *rho, double *ux,
                    double *uy, cudaStream_t s);
@@ -51,8 +54,15 @@ void launch_moments(const DevLattice &d, int view, int cur, int side_par, double
 // acc[0..lx*ly) += ux, acc[lx*ly..2*lx*ly) += uy of the current state.
 void launch_accumulate_velocity(const DevLattice &d, int view, int cur, int side_par, double *acc,
                                 cudaStream_t s);
+// max over the interior of |u - u_prev| into *out (float bits, cleared by the caller);
+// prev (lx*ly float2, [Y-1][X-1]) receives the current velocity.
+void launch_velocity_change(const DevLattice &d, int view, int cur, int side_par, void *prev,
+                            unsigned *out, cudaStream_t s);
 // ---- batches: many lattices per launch ------------------------------------------------
-constexpr int BATCH_THREADS = 128;
+// threads per block = nodes per tile: 128, 256 or 512
+// Kinds of batch step: pull (one node per thread), AA even and odd, and the 16-bit pull with four
+// nodes per thread (each warp one row of 128 nodes, see pull_quad).
+enum { BATCH_PULL = 0, BATCH_AA_EVEN = 1, BATCH_AA_ODD = 2, BATCH_PULL4 = 3 };
 
 // One lattice of a batch, with its state at the start of the current chunk of steps:
 // pull scheme: the buffer holding C_n is buf[cur0]; AA: phase0 0 = natural form, 1 = swapped;
@@ -68,17 +78,19 @@ struct BatchInst {
     int scheme, cur0, phase0, tau0;
 };
 
-// A tile of a lattice: nodes x0 .. x0 + tw - 1 and y0 .. y0 + (128/tw << r) - 1,
-// tw = 32 << (shape & 3), r = shape >> 2.
+// A tile of a lattice: nodes x0 .. x0 + (32 << shape) - 1 and y0 .. y0 + threads / (32 << shape) - 1
+// (BATCH_PULL4: x0 .. x0 + 127 and y0 .. y0 + threads / 32 - 1).
 struct BatchWork {
     int inst, x0, y0, shape;
 };
 
-// Step k of a chunk for every lattice of one scheme in the batch; `grid` blocks walk the work
-// list (one list per scheme, each kernel specialised for its scheme).
-void launch_batch(int precision, int scheme, const BatchInst *insts, const BatchWork *work,
-                  const int *nwork, int grid, int k, cudaStream_t s);
-int batch_blocks_per_sm(int precision, int scheme);
+// Step k of a chunk, of kind BATCH_PULL / AA_EVEN / AA_ODD / PULL4 (16-bit only), for every tile of a
+// work list of `nwork` tiles of `threads` nodes: `persistent` grids of `grid` blocks stride
+// through the list, otherwise `grid` must equal nwork (one block per tile).
+void launch_batch(int precision, int kind, int threads, bool persistent, const BatchInst *insts,
+                  const BatchWork *work, int nwork, int grid, int k, cudaStream_t s);
+// Resident blocks per SM of the persistent kernel of a kind and block size.
+int batch_blocks_per_sm(int precision, int kind, int threads);
 
 // AA scheme (buffer 0): the even step collides every node in place into the opposite slots,
 // the odd step gathers from the neighbours' opposite slots and scatters to their natural slots.

@@ -30,6 +30,27 @@ void zgb_slots_from_rows(const Lattice &L, const uint8_t *zgb_row, std::vector<i
         }
 }
 
+bool zgb_wanted(const uint8_t *zgb_row, int ly)
+{
+    if (zgb_row)
+        for (int Y = 0; Y < ly + 2; ++Y)
+            if (zgb_row[Y]) return true;
+    return false;
+}
+
+// Boundary tables, ZGB slots and omega of a geometry whose tags are already on the device.
+int set_tables(Lattice &L, double omega, const double *bc, const uint8_t *zgb_row)
+{
+    std::vector<int> src;
+    bool any = false;
+    zgb_slots_from_rows(L, zgb_row, src, any);
+    if (int rc = L.upload_bc(bc)) return rc;
+    if (int rc = L.upload_zgb_src(src.data())) return rc;
+    L.zgb_each_step = any;
+    L.d.omega = omega;
+    return LB_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -86,16 +107,10 @@ int lbgpu_set_geometry(lbgpu_lattice *h, double omega, const uint8_t *tag, const
     if (int rc = bad_handle(h, "lbgpu_set_geometry")) return rc;
     if (!tag || !bc) return set_error(LB_ERR_ARG, "lbgpu_set_geometry: null tag or table");
     Lattice &L = h->L;
-    std::vector<int> src;
-    bool any = false;
-    zgb_slots_from_rows(L, zgb_row, src, any);
-    if (any && L.lx < 2) return set_error(LB_ERR_ARG, "extrapolated outlet needs lx >= 2");
+    if (zgb_wanted(zgb_row, L.ly) && L.lx < 2)
+        return set_error(LB_ERR_ARG, "extrapolated outlet needs lx >= 2");
     if (int rc = L.upload_tags(tag)) return rc;
-    if (int rc = L.upload_bc(bc)) return rc;
-    if (int rc = L.upload_zgb_src(src.data())) return rc;
-    L.zgb_each_step = any;
-    L.d.omega = omega;
-    return LB_OK;
+    return set_tables(L, omega, bc, zgb_row);
 }
 
 int lbgpu_set_offset_scale(lbgpu_lattice *h, int scale_log2)
@@ -153,14 +168,19 @@ int lbgpu_setup_cylinder(lbgpu_lattice *h, int obst_x, int obst_y, int obst_r, d
 {
     if (int rc = bad_handle(h, "lbgpu_setup_cylinder")) return rc;
     Lattice &L = h->L;
-    const size_t nodes = (size_t)(L.lx + 2) * (L.ly + 2);
-    std::vector<uint8_t> tag(nodes), zgb(L.ly + 2);
+    // the tag plane is written on the device (O(nodes)); the boundary tables, O(perimeter),
+    // come from the host builder
+    std::vector<uint8_t> zgb(L.ly + 2);
     std::vector<double> bc(16 * (size_t)L.d.g.nb);
     const double omega = lbgpu_build_cylinder(L.lx, L.ly, obst_x, obst_y, obst_r, umax, re,
-                                              wall_kind, outlet_kind, tag.data(), bc.data(),
+                                              wall_kind, outlet_kind, nullptr, bc.data(),
                                               zgb.data(), nullptr);
     if (omega_out) *omega_out = omega;
-    if (int rc = lbgpu_set_geometry(h, omega, tag.data(), bc.data(), zgb.data())) return rc;
+    if (zgb_wanted(zgb.data(), L.ly) && L.lx < 2)
+        return set_error(LB_ERR_ARG, "extrapolated outlet needs lx >= 2");
+    lbgpu::launch_cylinder_tags(L.d, obst_x, obst_y, obst_r, wall_kind, L.stream);
+    if (int rc = lbgpu::cuda_error(cudaGetLastError(), "cylinder tags")) return rc;
+    if (int rc = set_tables(L, omega, bc.data(), zgb.data())) return rc;
     L.launches = 0;
     for (int b = 0; b < 2; ++b)
         if (L.d.buf[b])

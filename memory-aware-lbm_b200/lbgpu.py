@@ -46,6 +46,20 @@ class DriverConfig(ctypes.Structure):
                 ("variant", ctypes.c_int), ("blk", ctypes.c_int), ("sync_mode", ctypes.c_int)]
 
 
+class Request(ctypes.Structure):
+    _fields_ = [("lx", ctypes.c_int), ("ly", ctypes.c_int), ("obst_x", ctypes.c_int),
+                ("obst_y", ctypes.c_int), ("obst_r", ctypes.c_int), ("umax", ctypes.c_double),
+                ("re", ctypes.c_double), ("max_steps", ctypes.c_int), ("tol", ctypes.c_double),
+                ("arrival", ctypes.c_double), ("want_fields", ctypes.c_int)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("arrival", ctypes.c_double), ("admit", ctypes.c_double),
+                ("finish", ctypes.c_double), ("steps", ctypes.c_longlong),
+                ("nodes", ctypes.c_longlong), ("converged", ctypes.c_int),
+                ("done", ctypes.c_int), ("last_change", ctypes.c_double)]
+
+
 _LIB = None
 
 
@@ -96,10 +110,28 @@ def lib():
     L.lbgpu_batch_set_shape.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.lbgpu_batch_get_shape.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_int)]
+    L.lbgpu_batch_set_persistent.argtypes = [_vp, ctypes.c_int]
+    L.lbgpu_batch_get_persistent.argtypes = [_vp]
+    L.lbgpu_batch_set_threads.argtypes = [_vp, ctypes.c_int]
+    L.lbgpu_batch_get_threads.argtypes = [_vp]
     L.lbgpu_batch_autotune.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     L.lbgpu_tune_scheme.argtypes = [ctypes.c_int] * 4 + [ctypes.POINTER(ctypes.c_int),
                                                          ctypes.POINTER(ctypes.c_float),
                                                          ctypes.POINTER(ctypes.c_float)]
+    L.lbgpu_lattice_bytes.restype = ctypes.c_size_t
+    L.lbgpu_lattice_bytes.argtypes = [ctypes.c_int] * 4
+    L.lbgpu_server_create.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.c_int,
+                                      ctypes.POINTER(_vp)]
+    L.lbgpu_server_destroy.argtypes = [_vp]
+    L.lbgpu_server_set_scheme.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
+    L.lbgpu_server_set_shape.argtypes = [_vp] + [ctypes.c_int] * 3
+    L.lbgpu_server_set_persistent.argtypes = [_vp, ctypes.c_int]
+    L.lbgpu_server_set_threads.argtypes = [_vp, ctypes.c_int]
+    L.lbgpu_server_set_offset_scale.argtypes = [_vp, ctypes.c_int]
+    L.lbgpu_server_submit.argtypes = [_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int)]
+    L.lbgpu_server_run.argtypes = [_vp, ctypes.c_int]
+    L.lbgpu_server_result.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(Result), _dp, _dp]
+    L.lbgpu_server_stats.argtypes = [_vp, _dp]
     L.lbgpu_stream.restype = _vp
     L.lbgpu_stream.argtypes = [_vp]
     L.lbgpu_steps_done.restype = ctypes.c_longlong
@@ -369,13 +401,31 @@ class Batch:
     def last_launches(self):
         return lib().lbgpu_batch_last_launches(self.h)
 
-    def set_shape(self, size_class, tile_width, rows_per_thread):
-        _check(lib().lbgpu_batch_set_shape(self.h, size_class, tile_width, rows_per_thread))
+    def set_shape(self, size_class, tile_width, nodes_per_thread=1):
+        _check(lib().lbgpu_batch_set_shape(self.h, size_class, tile_width, nodes_per_thread))
 
     def shape(self, size_class):
-        w, r = ctypes.c_int(), ctypes.c_int()
-        _check(lib().lbgpu_batch_get_shape(self.h, size_class, ctypes.byref(w), ctypes.byref(r)))
-        return w.value, r.value
+        """(tile width, nodes per thread) of a size class."""
+        w, n = ctypes.c_int(), ctypes.c_int()
+        _check(lib().lbgpu_batch_get_shape(self.h, size_class, ctypes.byref(w), ctypes.byref(n)))
+        return w.value, n.value
+
+    @property
+    def persistent(self):
+        return bool(lib().lbgpu_batch_get_persistent(self.h))
+
+    @persistent.setter
+    def persistent(self, on):
+        _check(lib().lbgpu_batch_set_persistent(self.h, int(bool(on))))
+
+    @property
+    def threads(self):
+        """Threads per tile (= nodes per tile)."""
+        return lib().lbgpu_batch_get_threads(self.h)
+
+    @threads.setter
+    def threads(self, n):
+        _check(lib().lbgpu_batch_set_threads(self.h, int(n)))
 
     def autotune(self, steps=4):
         best = (ctypes.c_float * 6)()
@@ -393,3 +443,80 @@ def tune_scheme(precision, lx, ly, steps=10):
     _check(lib().lbgpu_tune_scheme(PRECISIONS[precision], lx, ly, steps, ctypes.byref(s),
                                    ctypes.byref(a), ctypes.byref(b)))
     return ("aa" if s.value == 1 else "pull"), a.value, b.value
+
+
+def lattice_bytes(lx, ly, precision="f32", scheme="pull"):
+    return lib().lbgpu_lattice_bytes(lx, ly, PRECISIONS[precision], SCHEMES[scheme])
+
+
+class Server:
+    """lbgpu_server: continuous batching of cylinder-channel requests under an HBM budget."""
+
+    def __init__(self, precision="f32", budget_bytes=8 << 30, check_every=100, scale=None):
+        self.precision = precision
+        h = _vp()
+        _check(lib().lbgpu_server_create(PRECISIONS[precision], int(budget_bytes),
+                                         int(check_every), ctypes.byref(h)))
+        self.h = h
+        self.requests = []
+        if precision in DEFAULT_SCALE:
+            _check(lib().lbgpu_server_set_offset_scale(
+                h, DEFAULT_SCALE[precision] if scale is None else int(scale)))
+
+    def close(self):
+        if self.h:
+            lib().lbgpu_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_scheme(self, size_class, scheme):
+        _check(lib().lbgpu_server_set_scheme(self.h, int(size_class), SCHEMES[scheme]))
+
+    def set_shape(self, size_class, tile_width, nodes_per_thread=1):
+        _check(lib().lbgpu_server_set_shape(self.h, int(size_class), int(tile_width),
+                                            int(nodes_per_thread)))
+
+    def set_persistent(self, on):
+        _check(lib().lbgpu_server_set_persistent(self.h, int(bool(on))))
+
+    def set_threads(self, n):
+        _check(lib().lbgpu_server_set_threads(self.h, int(n)))
+
+    def submit(self, lx, ly, obst_x, obst_y, obst_r, umax, re, max_steps, tol=0.0, arrival=0.0,
+               want_fields=False):
+        r = Request(lx, ly, obst_x, obst_y, obst_r, umax, re, max_steps, tol, arrival,
+                    int(want_fields))
+        i = ctypes.c_int()
+        _check(lib().lbgpu_server_submit(self.h, ctypes.byref(r), ctypes.byref(i)))
+        self.requests.append(r)
+        return i.value
+
+    def run(self, batched=True):
+        _check(lib().lbgpu_server_run(self.h, int(bool(batched))))
+
+    def result(self, rid, fields=False):
+        """dict of the request's record; with fields=True also (ux, uy) arrays [Y, X]."""
+        res = Result()
+        r = self.requests[rid]
+        ux = uy = None
+        if fields:
+            ux = np.zeros((r.ly, r.lx))
+            uy = np.zeros((r.ly, r.lx))
+        _check(lib().lbgpu_server_result(self.h, int(rid), ctypes.byref(res),
+                                         None if ux is None else _p(ux),
+                                         None if uy is None else _p(uy)))
+        out = {k: getattr(res, k) for k, _ in Result._fields_}
+        if fields:
+            out["ux"], out["uy"] = ux, uy
+        return out
+
+    def stats(self):
+        o = (ctypes.c_double * 4)()
+        _check(lib().lbgpu_server_stats(self.h, o))
+        return {"makespan_s": o[0], "lattice_updates": o[1], "peak_resident": int(o[2]),
+                "peak_bytes": int(o[3])}

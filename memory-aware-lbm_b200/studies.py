@@ -1,0 +1,277 @@
+"""Workload studies behind `bench.py --study`: batching, serving and storage precision.
+
+Every number comes from the library's kernels through lbgpu.py; the inputs are seeded synthetic
+cylinder channels (bounce-back walls, Poiseuille inlet, constant-density outlet).
+
+batching   independent channels of uneven size, Reynolds number and obstacle placement stepped
+           together (one persistent launch per step, CUDA-graph chunks of 50 steps, tile shapes
+           and pull/AA chosen per size class by the autotuners) against a sequential loop that
+           steps each channel alone with its own launches.
+serving    a Poisson stream of channel requests through lbgpu_server: continuous batching under
+           an HBM budget against sequential plain solves of the same requests; p50/p99 latency,
+           aggregate MLUPS, and the velocity error of a sample against FP64 re-runs.
+precision  one large channel stored as FP16 or BF16 offsets against the FP64 kernel: relative
+           L2 error of the time-averaged velocity, mass drift, drag and lift coefficients.
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+
+import lbgpu
+
+BYTES_PER_UPDATE = lbgpu.BYTES_PER_UPDATE
+
+
+def _pct(xs, q):
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
+
+
+# ------------------------------------------------------------------------------------------
+# batching
+# ------------------------------------------------------------------------------------------
+def batching_instances(n=512, seed=20260101):
+    """Channels with nx ~ U{64..2048 step 32}, ny ~ U{32..512 step 32}, Re ~ U[20, 200],
+    uMax ~ U[0.01, 0.04], radius ny/10 * U[0.8, 1.2], centre (nx/5, ny/2) * U[0.9, 1.1]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nx = 32 * int(rng.integers(2, 65))
+        ny = 32 * int(rng.integers(1, 17))
+        re = float(rng.uniform(20, 200))
+        umax = float(rng.uniform(0.01, 0.04))
+        r = max(2, int(round(ny / 10 * rng.uniform(0.8, 1.2))))
+        ox = min(nx - r - 2, max(r + 2, int(round(nx / 5 * rng.uniform(0.9, 1.1))) + 1))
+        oy = min(ny - r - 1, max(r + 2, int(round(ny / 2 * rng.uniform(0.9, 1.1))) + 1))
+        out.append(dict(lx=nx, ly=ny, obst_x=ox, obst_y=oy, obst_r=r, umax=umax, re=re))
+    return out
+
+
+def _channel(q, precision, scheme):
+    lat = lbgpu.Lattice(q["lx"], q["ly"], precision, scheme)
+    if precision in lbgpu.DEFAULT_SCALE:
+        lat.set_offset_scale(lbgpu.DEFAULT_SCALE[precision])
+    lat.setup_cylinder(q["obst_x"], q["obst_y"], q["obst_r"], q["umax"], q["re"],
+                       lbgpu.WALL_BOUNCEBACK, lbgpu.OUTLET_CONST)
+    return lat
+
+
+def tune_schemes(precision, sizes, steps=6):
+    """Pull or AA per size class, timed on the median-sized lattice of each class present."""
+    by_class = {}
+    for lx, ly in sizes:
+        by_class.setdefault(lbgpu.size_class(lx * ly), []).append((lx * ly, lx, ly))
+    out = {}
+    for c, members in sorted(by_class.items()):
+        members.sort()
+        _, lx, ly = members[len(members) // 2]
+        scheme, t_pull, t_aa = lbgpu.tune_scheme(precision, lx, ly, steps)
+        out[c] = {"scheme": scheme, "probe": [lx, ly], "ms_pull": round(t_pull, 4),
+                  "ms_aa": round(t_aa, 4)}
+    return out
+
+
+def batching_study(precisions=("f32", "f16"), n=512, steps=2000, seed=20260101):
+    insts = batching_instances(n, seed)
+    nodes = sum(q["lx"] * q["ly"] for q in insts)
+    res = {"instances": n, "seed": seed, "nodes": nodes, "steps": steps, "chunk": 50,
+           "precisions": {}}
+    for prec in precisions:
+        schemes = tune_schemes(prec, [(q["lx"], q["ly"]) for q in insts])
+        lats = [_channel(q, prec, schemes[lbgpu.size_class(q["lx"] * q["ly"])]["scheme"])
+                for q in insts]
+        try:
+            with lbgpu.Batch(prec) as b:
+                slots = [b.add(l) for l in lats]
+                best = b.autotune(4)
+                shapes = {c: list(b.shape(c)) for c in schemes}
+                persistent = b.persistent
+                threads = b.threads
+                b.step(50)                     # first-step path and the graph capture
+                b.synchronize()
+                t0 = time.perf_counter()
+                ms = b.step_timed(steps)
+                wall_b = time.perf_counter() - t0
+                launches = b.last_launches
+                for s in slots:
+                    b.remove(s)
+            for l in lats:                     # the sequential loop, warmed the same way
+                l.step(3)
+            for l in lats:
+                l.synchronize()
+            t0 = time.perf_counter()
+            for l in lats:
+                l.step(steps)
+            for l in lats:
+                l.synchronize()
+            wall_s = time.perf_counter() - t0
+        finally:
+            for l in lats:
+                l.close()
+        mb = nodes * steps / (ms * 1e-3) / 1e6
+        mbw = nodes * steps / wall_b / 1e6
+        msq = nodes * steps / wall_s / 1e6
+        res["precisions"][prec] = {
+            "batched_mlups": round(mb, 1), "batched_mlups_wall": round(mbw, 1),
+            "batched_kernel_launches": launches,
+            "sequential_mlups_wall": round(msq, 1), "speedup_wall": round(mbw / msq, 2),
+            "batched_gbs_algorithmic": round(mb * 1e6 * BYTES_PER_UPDATE[prec] / 1e9, 1),
+            "schemes": {str(k): v for k, v in schemes.items()},
+            "tile_shapes": {str(k): v for k, v in shapes.items()},
+            "persistent": persistent, "threads_per_tile": threads,
+            "autotune_best_ms": [round(x, 4) for x in best]}
+    return res
+
+
+# ------------------------------------------------------------------------------------------
+# serving
+# ------------------------------------------------------------------------------------------
+def serving_requests(n, seed=20260102, nmin=1e4, nmax=2e7, max_steps=5000, tol=1e-7,
+                     umax=0.02):
+    """Node counts log-uniform on [nmin, nmax], aspect nx/ny ~ U[2, 8], Re ~ U[20, 500];
+    obstacle at (nx/5 + 1, ny/2 + 1), radius ny/10 + 1; arrival times are set later."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        N = math.exp(rng.uniform(math.log(nmin), math.log(nmax)))
+        aspect = rng.uniform(2, 8)
+        ny = max(16, int(round(math.sqrt(N / aspect))))
+        nx = max(32, int(round(N / ny)))
+        r = ny // 10 + 1
+        out.append(dict(lx=nx, ly=ny, obst_x=nx // 5 + 1, obst_y=ny // 2 + 1, obst_r=r,
+                        umax=umax, re=float(rng.uniform(20, 500)), max_steps=max_steps,
+                        tol=tol, arrival=0.0, want_fields=False))
+    return out
+
+
+def _serve(prec, reqs, batched, budget, schemes=None, shapes=None, sample=()):
+    with lbgpu.Server(prec, budget, 100) as srv:
+        for c, s in (schemes or {}).items():
+            srv.set_scheme(c, s)
+        for c, (w, npt) in (shapes or {}).items():
+            srv.set_shape(c, w, npt)
+        for k, q in enumerate(reqs):
+            srv.submit(**dict(q, want_fields=k in sample))
+        srv.run(batched)
+        res = [srv.result(k, fields=k in sample) for k in range(len(reqs))]
+        st = srv.stats()
+    lat = [r["finish"] - r["arrival"] for r in res]
+    return {"makespan_s": round(st["makespan_s"], 3),
+            "mlups": round(st["lattice_updates"] / st["makespan_s"] / 1e6, 1),
+            "p50_latency_s": round(_pct(lat, 50), 4), "p99_latency_s": round(_pct(lat, 99), 4),
+            "mean_latency_s": round(float(np.mean(lat)), 4),
+            "peak_resident": st["peak_resident"], "peak_gb": round(st["peak_bytes"] / 1e9, 2),
+            "converged": sum(1 for r in res if r["converged"] == 1),
+            "diverged": sum(1 for r in res if r["converged"] == -1)}, res
+
+
+def serving_study(precisions=("f32", "f16"), n=120, seed=20260102, budget_gb=150.0,
+                  load=0.95, sample_every=50):
+    reqs = serving_requests(n, seed)
+    work = [q["lx"] * q["ly"] * q["max_steps"] for q in reqs]
+    budget = int(budget_gb * 1e9)
+    sample = set(range(0, n, sample_every))
+    out = {"requests": n, "seed": seed, "budget_gb": budget_gb, "offered_load": load,
+           "nodes_log_uniform": [1e4, 2e7], "max_steps": 5000, "tol": 1e-7,
+           "fp64_sample": sorted(sample), "precisions": {}}
+    rng = np.random.default_rng(seed + 1)
+    # FP64 re-runs of the sample (alone, same step counts) are made after the served runs
+    for prec in precisions:
+        schemes = {c: v["scheme"] for c, v in
+                   tune_schemes(prec, [(q["lx"], q["ly"]) for q in reqs]).items()}
+        # capacity: the batched rate on the whole request set at once (all arrive at t=0)
+        closed, _ = _serve(prec, reqs, True, budget, schemes)
+        cap = closed["mlups"] * 1e6
+        mean_work = float(np.mean(work))
+        rate = load * cap / mean_work            # requests per second
+        t = np.cumsum(rng.exponential(1.0 / rate, n))
+        stream = [dict(q, arrival=float(t[k] - t[0])) for k, q in enumerate(reqs)]
+        served, res = _serve(prec, stream, True, budget, schemes, sample=sample)
+        # sequential plain solves: each request alone with the single-lattice pull kernel
+        seq, _ = _serve(prec, stream, False, budget)
+        seq_closed, _ = _serve(prec, reqs, False, budget)
+        errs = []
+        for k in sorted(sample):
+            q = reqs[k]
+            with _channel(q, "f64", "pull") as lat:
+                lat.step(res[k]["steps"])
+                _, ux, uy = lat.macros()
+            du = np.hypot(res[k]["ux"] - ux, res[k]["uy"] - uy)
+            errs.append(float(np.linalg.norm(du) / max(np.linalg.norm(np.hypot(ux, uy)), 1e-300)))
+        out["precisions"][prec] = {
+            "schemes": {str(k): v for k, v in schemes.items()},
+            "arrival_rate_per_s": round(rate, 3),
+            "closed_batched": closed, "closed_sequential": seq_closed,
+            "stream_batched": served, "stream_sequential": seq,
+            "throughput_ratio_closed": round(closed["mlups"] / seq_closed["mlups"], 2),
+            "velocity_rel_l2_vs_fp64": {"max": max(errs), "median": float(np.median(errs)),
+                                        "n": len(errs)}}
+    # sequential plain FP64 solves of the same requests, all present at t = 0
+    plain, _ = _serve("f64", reqs, False, budget)
+    out["closed_sequential_f64_plain"] = plain
+    for prec in precisions:
+        p = out["precisions"][prec]
+        p["throughput_ratio_vs_f64_plain"] = round(p["closed_batched"]["mlups"] / plain["mlups"], 2)
+    return out
+
+
+# ------------------------------------------------------------------------------------------
+# precision
+# ------------------------------------------------------------------------------------------
+def _run_averaged(nx, ny, prec, umax, re, steps, avg_every, moment_every):
+    ox, oy, r = nx // 5 + 1, ny // 2 + 1, ny // 10 + 1
+    q = dict(lx=nx, ly=ny, obst_x=ox, obst_y=oy, obst_r=r, umax=umax, re=re)
+    with _channel(q, prec, "pull") as lat:
+        m0 = lat.moments()
+        half = steps // 2
+        ms = lat.step_timed(half)
+        fx, fy = [], []
+        done = half
+        while done < steps:
+            k = min(avg_every, steps - done)
+            ms += lat.step_timed(k)
+            done += k
+            lat.velocity_accumulate()
+            if done % moment_every == 0:
+                m = lat.moments()
+                fx.append(m[3])
+                fy.append(m[4])
+        m1 = lat.moments()
+        ux, uy, nsamp = lat.velocity_average()
+    u_mean = 2.0 / 3.0 * umax                 # mean of the Poiseuille inflow profile
+    dyn = 0.5 * 1.0 * u_mean ** 2 * (2 * r)
+    return {"ux": ux, "uy": uy, "samples": nsamp, "mass0": m0[0], "mass1": m1[0],
+            "non_finite": int(m1[6]), "cd": float(np.mean(fx)) / dyn, "cl": float(np.mean(fy)) / dyn,
+            "cl_rms": float(np.sqrt(np.mean(np.square(fy)))) / dyn,
+            "mlups": nx * ny * steps / (ms * 1e-3) / 1e6}
+
+
+def precision_study(nx=16384, ny=4096, steps=20000, cases=((100.0, 0.02), (1000.0, 0.05)),
+                    precisions=("f16", "bf16"), avg_every=10, moment_every=100):
+    out = {"nx": nx, "ny": ny, "steps": steps, "average": f"every {avg_every} steps over the "
+           f"second half", "forces": f"momentum exchange every {moment_every} steps over the "
+           "second half; C = F / (0.5 rho U^2 D), U = 2/3 uMax, D = 2r", "cases": []}
+    for re, umax in cases:
+        ref = _run_averaged(nx, ny, "f64", umax, re, steps, avg_every, moment_every)
+        nref = float(np.sqrt(np.sum(ref["ux"] ** 2 + ref["uy"] ** 2)))
+        case = {"re": re, "umax": umax,
+                "f64": {"mlups": round(ref["mlups"], 1), "cd": ref["cd"], "cl": ref["cl"],
+                        "cl_rms": ref["cl_rms"],
+                        "mass_drift": (ref["mass1"] - ref["mass0"]) / ref["mass0"],
+                        "non_finite": ref["non_finite"]}}
+        for prec in precisions:
+            r = _run_averaged(nx, ny, prec, umax, re, steps, avg_every, moment_every)
+            err = float(np.sqrt(np.sum((r["ux"] - ref["ux"]) ** 2 + (r["uy"] - ref["uy"]) ** 2))) / nref
+            case[prec] = {"mlups": round(r["mlups"], 1), "vel_rel_l2_time_avg": err,
+                          "mass_drift": (r["mass1"] - r["mass0"]) / r["mass0"],
+                          "cd": r["cd"], "cl": r["cl"], "cl_rms": r["cl_rms"],
+                          "cd_rel_err": abs(r["cd"] - ref["cd"]) / abs(ref["cd"]),
+                          "cl_abs_err": abs(r["cl"] - ref["cl"]),
+                          "non_finite": r["non_finite"],
+                          "scale_log2": lbgpu.DEFAULT_SCALE[prec]}
+            del r
+        out["cases"].append(case)
+        del ref
+    return out

@@ -149,6 +149,9 @@ def test_errors_are_reported_not_raised_without_a_device():
     with pytest.raises(lbgpu.LbError) as e:
         lbgpu.drive(20, 10, 5, 6, 2, 2, "origin")
     assert e.value.code == 8
+    with pytest.raises(lbgpu.LbError) as e:
+        lbgpu.Server("f32", 1 << 20, 100)
+    assert e.value.code == 8
 
 
 def test_bad_arguments_are_rejected():
@@ -164,6 +167,14 @@ def test_bad_arguments_are_rejected():
         lbgpu.drive(-1, 10, 5, 6, 2, 2, "origin")
     assert e.value.code == 3
     lbgpu.clear_error()
+    s = ctypes.c_void_p()
+    assert L.lbgpu_server_create(1, 1 << 20, 0, ctypes.byref(s)) == 3   # check interval 0
+    assert L.lbgpu_server_create(7, 1 << 20, 100, ctypes.byref(s)) == 3  # no such precision
+    lbgpu.clear_error()
+    # the admission estimate is the sum of the lattice's allocations (two buffers vs one)
+    pull = lbgpu.lattice_bytes(250, 51, "f32", "pull")
+    aa = lbgpu.lattice_bytes(250, 51, "f32", "aa")
+    assert pull > aa > 9 * 4 * 250 * 51
 
 
 @pytest.mark.skipif(not O.ref_available(), reason="reference build oracle/_ref not present")

@@ -83,9 +83,10 @@ def test_autotuned_shapes_keep_results_exact():
         best = b.autotune(2)
         classes = {lbgpu.size_class(lx * ly) for lx, ly in SIZES[:3]}
         for c in classes:
-            w, r = b.shape(c)
-            assert w in (32, 64, 128) and r in (1, 2, 4)
+            assert b.shape(c) in ((32, 1), (64, 1), (128, 1))
             assert best[c] > 0
+        assert all(best[c] == 0 for c in range(6) if c not in classes)
+        assert b.threads in (128, 256, 512)
         b.step(7)
         b.synchronize()
         got = [(l.populations(), l.steps_done) for l in lats]
@@ -98,10 +99,69 @@ def test_autotuned_shapes_keep_results_exact():
         l.close()
 
 
+@pytest.mark.parametrize("persistent,width,threads", [
+    (True, 128, 128), (False, 128, 128), (True, 32, 128), (False, 64, 128),
+    (True, 64, 256), (False, 32, 256), (True, 128, 512), (False, 32, 512)])
+def test_every_launch_form_and_tile_is_exact(persistent, width, threads):
+    """AA members that join at different phases run as two lists of opposite kinds."""
+    lats = [channel(lx, ly, "f32", s, k) for k, ((lx, ly), s) in
+            enumerate(zip(SIZES[:4], ["aa", "pull", "aa", "aa"]))]
+    lats[2].step(1)                    # an AA member in the swapped phase when it joins
+    with lbgpu.Batch("f32") as b:
+        b.persistent = persistent
+        b.threads = threads
+        assert b.persistent == persistent and b.threads == threads
+        for c in range(6):
+            b.set_shape(c, width, 1)
+        slots = [b.add(l) for l in lats]
+        for n in (51, 50, 3):          # odd rest: the lists swap kinds; then a graph again
+            b.step(n)
+        b.synchronize()
+        got = [(l.populations(), l.steps_done) for l in lats]
+        for s in slots:
+            b.remove(s)
+    for k, ((lx, ly), s) in enumerate(zip(SIZES[:4], ["aa", "pull", "aa", "aa"])):
+        pops, steps = got[k]
+        assert same(pops, alone(lx, ly, "f32", s, k, steps)), (k, s, persistent, width)
+    for l in lats:
+        l.close()
+
+
+@pytest.mark.parametrize("precision", ["f16", "bf16"])
+@pytest.mark.parametrize("persistent,threads", [(True, 128), (False, 256), (False, 512)])
+def test_four_nodes_a_thread_is_exact(precision, persistent, threads):
+    """16-bit pull members in quad tiles (narrow ones fall back to per-node) beside AA members."""
+    sizes = [(300, 40), (257, 35), (96, 40), (520, 70)]
+    schemes = ["pull", "pull", "pull", "aa"]
+    lats = [channel(lx, ly, precision, s, k) for k, ((lx, ly), s) in enumerate(zip(sizes, schemes))]
+    with lbgpu.Batch(precision) as b:
+        b.persistent = persistent
+        b.threads = threads
+        for c in range(6):
+            b.set_shape(c, 128, 4)
+            assert b.shape(c) == (128, 4)
+        slots = [b.add(l) for l in lats]
+        for n in (3, 50, 7):
+            b.step(n)
+        b.synchronize()
+        got = [(l.populations(), l.steps_done) for l in lats]
+        for s in slots:
+            b.remove(s)
+    for k, ((lx, ly), s) in enumerate(zip(sizes, schemes)):
+        pops, steps = got[k]
+        assert same(pops, alone(lx, ly, precision, s, k, steps)), (k, s, persistent, threads)
+    for l in lats:
+        l.close()
+
+
 def test_batch_rejects_mismatched_members():
     with lbgpu.Batch("f32") as b, lbgpu.Lattice(40, 20, "f64") as wrong:
         with pytest.raises(lbgpu.LbError) as e:
             b.add(wrong)
+        assert e.value.code == 3
+    with lbgpu.Batch("f32") as b:
+        with pytest.raises(lbgpu.LbError) as e:
+            b.set_shape(0, 128, 4)             # four nodes a thread: 16-bit storage only
         assert e.value.code == 3
     with lbgpu.Batch("f64") as b, lbgpu.Lattice(40, 20, "f64") as zgb:
         zgb.setup_cylinder(9, 11, 3, 0.02, 100.0, lbgpu.WALL_REGULARIZED, lbgpu.OUTLET_ZGB)
