@@ -53,7 +53,8 @@ def parse():
     p.add_argument("--nx", type=int, default=16384)
     p.add_argument("--ny", type=int, default=4096)
     p.add_argument("--precision", default="f64", choices=list(BYTES_PER_UPDATE))
-    p.add_argument("--scheme", default="pull", choices=["pull", "aa"])
+    p.add_argument("--scheme", default="pull", choices=["pull", "aa", "pull2"],
+                   help="pull2: the pull scheme with two steps per sweep (temporal blocking)")
     p.add_argument("--variants", default="auto",
                    help="comma list of precision:scheme also timed, 'auto' or 'none'")
     p.add_argument("--study", choices=["batching", "serving", "precision"], default=None,
@@ -280,8 +281,10 @@ def run_reference_arm(args, dist):
 # ---------------------------------------------------------------------------------------
 def time_lattice(lbgpu, nx, ny, precision, scheme, steps, warmup, dist, sampler_dev=None):
     ox, oy, r = cylinder(nx, ny)
-    lat = lbgpu.Lattice(nx, ny, precision, scheme)
+    lat = lbgpu.Lattice(nx, ny, precision, "pull" if scheme == "pull2" else scheme)
     try:
+        if scheme == "pull2":
+            lat.set_sweep_steps(2)
         if precision in ("f16", "bf16"):   # the scale encodes the initial state: set it first
             lat.set_offset_scale(lbgpu_default_scale(precision))
         lat.setup_cylinder(ox, oy, r, 0.02, 100.0, lbgpu.WALL_BOUNCEBACK, lbgpu.OUTLET_CONST)
@@ -329,8 +332,8 @@ def run_ours(args, dist):
     variants = {}
     vlist = []
     if args.variants == "auto":
-        vlist = [("f64", "aa"), ("f32", "pull"), ("f32", "aa"), ("f16", "pull"), ("bf16", "pull"),
-                 ("f16", "aa")]
+        vlist = [("f64", "aa"), ("f64", "pull2"), ("f32", "pull"), ("f32", "aa"), ("f32", "pull2"),
+                 ("f16", "pull"), ("bf16", "pull"), ("f16", "aa"), ("f16", "pull2")]
     elif args.variants != "none":
         vlist = [tuple(v.split(":")) for v in args.variants.split(",") if v]
     for prec, sch in vlist:
@@ -344,6 +347,10 @@ def run_ours(args, dist):
                 "ms_per_step": round(vms / K, 4),
                 "gbs_algorithmic": round(vb * nodes / (vms * 1e-3 / K) / 1e9, 1),
                 "roofline_frac": round(vb * nodes / (vms * 1e-3 / K) / 1e9 / peak, 4)}
+            if sch == "pull2":   # its own algorithmic bytes: one read + one write per two steps
+                variants[f"{prec}_{sch}"]["own_bytes_per_update"] = vb // 2
+                variants[f"{prec}_{sch}"]["own_roofline_frac"] = round(
+                    vb / 2 * nodes / (vms * 1e-3 / K) / 1e9 / peak, 4)
         except Exception as e:  # a kernel family not built yet is reported, not hidden
             variants[f"{prec}_{sch}"] = {"error": str(e)[:200]}
 

@@ -129,6 +129,14 @@ double lbgpu_build_cylinder(int lx, int ly, int obst_x, int obst_y, int obst_r, 
                             double re, int wall_kind, int outlet_kind, uint8_t *tag,
                             double *bc, uint8_t *zgb_row, double *f);
 
+/* Steps per sweep of the pull scheme: 1 (default) or 2.  With 2, lbgpu_step advances pairs of
+ * steps in one kernel that keeps the intermediate state in shared memory (temporal blocking,
+ * the GPU form of the reference's collide_tight two-steps-per-sweep idea, lb.c:442-572): one
+ * read and one write of the lattice per two steps.  Results are identical to single steps.
+ * Lattices with an extrapolated outlet (a pass between every two steps) and the first step of
+ * a fresh lattice still run single steps.  LB_ERR_STATE for the AA scheme. */
+int lbgpu_set_sweep_steps(lbgpu_lattice *lat, int steps);
+
 /* Advance `nsteps` time steps; asynchronous on the lattice's stream. */
 int lbgpu_step(lbgpu_lattice *lat, int nsteps);
 
@@ -199,7 +207,7 @@ int lbgpu_batch_size_class(long long nodes);
 int lbgpu_batch_set_shape(lbgpu_batch *b, int size_class, int tile_width, int nodes_per_thread);
 int lbgpu_batch_get_shape(lbgpu_batch *b, int size_class, int *tile_width, int *nodes_per_thread);
 /* Launch form: 1 = a persistent grid (resident blocks per SM x SMs) strides through the work
- * list (the default), 0 = one block per tile. */
+ * list, 0 = one block per tile (the default). */
 int lbgpu_batch_set_persistent(lbgpu_batch *b, int persistent);
 int lbgpu_batch_get_persistent(lbgpu_batch *b);
 /* Threads per tile (= nodes per tile, one block per tile): 128 (default), 256 or 512. */

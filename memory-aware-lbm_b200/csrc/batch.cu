@@ -3,12 +3,13 @@
 // Every step of every member runs in at most four launches, one per kind of step: the pull step
 // of the two-buffer members (one node per thread, or for 16-bit storage optionally four nodes
 // per thread), and the even and the odd AA step of the in-place members (AA members are kept in
-// two lists by the parity of their phase, so each list runs one kind at a time).  A launch walks a work list of tiles (member, x0, y0, tile width) of 128, 256 or 512
-// nodes, one per thread: either a persistent grid of (blocks per SM x SMs) blocks strides
-// through it, or one block per tile.
-// Steps are grouped in chunks of 50 (an even count) captured once as a CUDA graph: the kernels
-// read each member's buffers and parities from a device descriptor array, so the same graph
-// replays chunk after chunk; it is re-captured when the membership or the launch form changes.
+// two lists by the parity of their phase, so each list runs one kind at a time).  A launch
+// walks a work list of tiles (member, x0, y0, shape) of 128, 256 or 512 nodes, one per thread
+// (or four per thread): either one block per tile, or a persistent grid of (blocks per SM x
+// SMs) blocks strides through it.  Steps are grouped in chunks of 50 (an even count) captured
+// once as a CUDA graph: the kernels read each member's buffers and parities from a device
+// descriptor array, so the same graph replays chunk after chunk; it is re-captured when the
+// membership or the launch form changes.
 // Tile widths are chosen per size class of member (node count), the threads per tile and the
 // launch form per batch, by hand or by lbgpu_batch_autotune.
 #include <algorithm>
@@ -48,7 +49,7 @@ struct lbgpu_batch {
     std::vector<lbgpu_lattice *> members;   // slot -> lattice (null: free slot)
     int shape[kClasses] = {2, 2, 2, 2, 2, 2};  // 0..2: 32 << shape wide; kQuad: 16-bit quad pull
     int threads = 128;                       // nodes per tile = threads per block
-    bool persistent = true;
+    bool persistent = false;
     BatchInst *d_inst = nullptr;
     int cap_inst = 0;
     BatchWork *d_work[kLists] = {nullptr, nullptr, nullptr, nullptr};

@@ -13,6 +13,7 @@
 //
 // Storage types: double (exact FP64 arithmetic), float, __half / __nv_bfloat16 offsets
 // (codec.cuh), all with the same index space (layout.cuh).
+#include <algorithm>
 #include "codec.cuh"
 #include "kernels.h"
 #include "lbgpu.h"
@@ -117,33 +118,39 @@ template <> struct Half2Ops<__nv_bfloat16> {
     }
 };
 
-// BGK on scaled offsets D[9] of one node.  Opposite directions i, opp(i) share cu (up to sign):
-// E_i, E_opp = a +- b with a = 2^s w (A + 4.5 rho cu^2), b = 2^s w 3 rho cu, A = rho(1-1.5u^2)-1.
+// BGK on scaled offsets D[9] of one node (sc = 2^s, inv = 2^-s).  With d = rho - 1 =
+// inv sum(D) and j = rho u = inv sum(c D), rho c.u = c.j and rho u^2 = j.u give
+//   E_i = sc w_i (A + 3 c.j + 4.5 (c.u)(c.j)),  A = d - 1.5 j.u,
+// and the relaxation is D_i' = (1 - omega) D_i + omega E_i.  Opposite directions i, opp(i)
+// share c.u and c.j up to sign: omega E_i, omega E_opp = a +- b with
+// a = k (A + 4.5 (c.u)(c.j)), b = 3 k c.j, k = omega sc w.
 // 1/rho uses the hardware reciprocal (the 16-bit path is held to a tolerance, not bit-exact).
 __device__ __forceinline__ void bgk_offsets(float D[9], float omega, float sc, float inv)
 {
+    // J = 2^s j (scaled sums): u = J inv / rho, and inv folds into the constants below
     const float sum = ((D[0] + D[1]) + (D[2] + D[3])) + ((D[4] + D[5]) + (D[6] + D[7])) + D[8];
-    const float rho = fmaf(inv, sum, 1.0f);
-    const float jx = inv * ((D[1] - D[3]) + (D[5] - D[6]) + (D[8] - D[7]));
-    const float jy = inv * ((D[2] - D[4]) + (D[5] - D[8]) + (D[6] - D[7]));
-    const float ir = __fdividef(1.0f, rho);
-    const float ux = jx * ir, uy = jy * ir;
-    const float A = fmaf(rho, fmaf(-1.5f, fmaf(ux, ux, uy * uy), 1.0f), -1.0f);
-    const float w1 = sc * (1.f / 9.f), w2 = sc * (1.f / 36.f);
-    D[0] = fmaf(omega, (sc * (4.f / 9.f)) * A - D[0], D[0]);
-#define LBGPU_PAIR(I, J, W, CU)                                        \
+    const float d = inv * sum;
+    const float Jx = (D[1] - D[3]) + (D[5] - D[6]) + (D[8] - D[7]);
+    const float Jy = (D[2] - D[4]) + (D[5] - D[8]) + (D[6] - D[7]);
+    const float q = inv * __fdividef(1.0f, 1.0f + d);
+    const float ux = Jx * q, uy = Jy * q;
+    const float A = fmaf(-1.5f * inv, fmaf(Jx, ux, Jy * uy), d);
+    const float ux45 = (4.5f * inv) * ux, uy45 = (4.5f * inv) * uy;
+    const float om1 = 1.0f - omega;
+    const float k0 = omega * sc * (4.f / 9.f), k1 = omega * sc * (1.f / 9.f), k2 = omega * sc * (1.f / 36.f);
+    D[0] = fmaf(om1, D[0], k0 * A);
+#define LBGPU_PAIR(I, J, K, CU45, CJ)                                  \
     {                                                                  \
-        const float cu = (CU);                                         \
-        const float rcu = rho * cu;                                    \
-        const float a = W * fmaf(4.5f * cu, rcu, A);                   \
-        const float b = (3.0f * W) * rcu;                              \
-        D[I] = fmaf(omega, (a + b) - D[I], D[I]);                      \
-        D[J] = fmaf(omega, (a - b) - D[J], D[J]);                      \
+        const float cj = (CJ);                                         \
+        const float a = K * fmaf(CU45, cj, A);                         \
+        const float b = ((3.0f * inv) * K) * cj;                       \
+        D[I] = fmaf(om1, D[I], a + b);                                 \
+        D[J] = fmaf(om1, D[J], a - b);                                 \
     }
-    LBGPU_PAIR(1, 3, w1, ux)
-    LBGPU_PAIR(2, 4, w1, uy)
-    LBGPU_PAIR(5, 7, w2, ux + uy)
-    LBGPU_PAIR(6, 8, w2, uy - ux)
+    LBGPU_PAIR(1, 3, k1, ux45, Jx)
+    LBGPU_PAIR(2, 4, k1, uy45, Jy)
+    LBGPU_PAIR(5, 7, k2, ux45 + uy45, Jx + Jy)
+    LBGPU_PAIR(6, 8, k2, uy45 - ux45, Jy - Jx)
 #undef LBGPU_PAIR
 }
 
@@ -282,13 +289,7 @@ __global__ void __launch_bounds__(BX) k_pull(Geo g, const S *__restrict__ src, S
     }
 }
 
-// Pull step for 16-bit storage, four nodes per thread (X = x0..x0+3, x0 = 1 + 4t, so a quad is
-// one aligned 8-byte word pair).  Interior warps: per direction one aligned 8-byte load, the
-// x-shifted quad assembled from the adjacent lane's word (one 32-bit shuffle) and byte
-// permutes; edge lanes take the neighbouring word from a second load whose address differs only
-// in that lane.  Warps touching the perimeter or the row's end run the per-node path.  The
-// kernel is bounded by instruction issue, so the collision is written for few instructions
-// (bgk_offsets) and the boundary rules stay out of line.
+// Pull step of one node, any storage type (the general path of every pull kernel).
 template <class S>
 __device__ __forceinline__ void pull_node(const Geo &g, const S *__restrict__ src, S *__restrict__ dst,
                                           const uint8_t *__restrict__ tag, const double *__restrict__ bc,
@@ -321,9 +322,16 @@ __device__ __forceinline__ void pull_node(const Geo &g, const S *__restrict__ sr
     }
 }
 
+// Pull step for 16-bit storage, four nodes per thread (X = x0..x0+3 with x0 = 1 mod 4, so a
+// quad is one aligned 8-byte word pair).  Interior warps: per direction one aligned 8-byte load;
+// an x-shifted quad is assembled by byte permutes from that word pair and the neighbouring
+// 4-byte word, loaded by every lane (the adjacent lane's data, so an L1 hit).  Warps touching
+// the perimeter or the row's end run the per-node path.  The kernel is bounded by instruction
+// issue, so the collision is written for few instructions (bgk_offsets) and the boundary rules
+// stay out of line.
 //
-// pull_quad runs the four nodes x0..x0+3 of row Y (x0 = 1 mod 4) for one lane of a warp whose
-// lanes cover 128 consecutive nodes; the whole warp must call it together (shuffles).
+// pull_quad runs the four nodes x0..x0+3 of row Y for one lane of a warp whose lanes cover 128
+// consecutive nodes (the choice between the vector and the per-node path is made per warp).
 template <class S>
 __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ src, S *__restrict__ dst,
                                           const uint8_t *__restrict__ tag, const double *__restrict__ bc,
@@ -345,8 +353,10 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
     for (int i = 0; i < 9; ++i) {
         const S *row = plane(src, g, i) + (o - (long long)cy(i) * g.pitch);
         v[i] = *reinterpret_cast<const uint2 *>(row);
-        if (cx(i) == 1) e[i] = *reinterpret_cast<const unsigned *>(lane == 0 ? row - 2 : row);
-        if (cx(i) == -1) e[i] = *reinterpret_cast<const unsigned *>(lane == 31 ? row + 4 : row);
+        // the word holding the shifted quad's outer source (the neighbouring lane's data:
+        // an L1 hit, no extra DRAM traffic, and no shuffle)
+        if (cx(i) == 1) e[i] = *reinterpret_cast<const unsigned *>(row - 2);
+        if (cx(i) == -1) e[i] = *reinterpret_cast<const unsigned *>(row + 4);
     }
     const unsigned tq = *reinterpret_cast<const unsigned *>(tag + o);
     float D[4][9];
@@ -354,14 +364,10 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
     for (int i = 0; i < 9; ++i) {
         unsigned w0 = v[i].x, w1 = v[i].y;
         if (cx(i) == 1) {            // quad of sources x0-1..x0+2
-            unsigned pw = __shfl_up_sync(0xffffffffu, v[i].y, 1);
-            if (lane == 0) pw = e[i];
-            const unsigned n0 = __byte_perm(pw, w0, 0x5432), n1 = __byte_perm(w0, w1, 0x5432);
+            const unsigned n0 = __byte_perm(e[i], w0, 0x5432), n1 = __byte_perm(w0, w1, 0x5432);
             w0 = n0; w1 = n1;
         } else if (cx(i) == -1) {    // quad of sources x0+1..x0+4
-            unsigned nw = __shfl_down_sync(0xffffffffu, v[i].x, 1);
-            if (lane == 31) nw = e[i];
-            const unsigned n0 = __byte_perm(w0, w1, 0x5432), n1 = __byte_perm(w1, nw, 0x5432);
+            const unsigned n0 = __byte_perm(w0, w1, 0x5432), n1 = __byte_perm(w1, e[i], 0x5432);
             w0 = n0; w1 = n1;
         }
         D[0][i] = H::lo(w0); D[1][i] = H::hi(w0);
@@ -385,8 +391,10 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
     }
 }
 
+// Eight blocks of 128 threads a SM (64 registers): more loads in flight than the 72-register
+// allocation's seven, for a few bytes of spills on the per-node fallback path.
 template <class S>
-__global__ void __launch_bounds__(BX) k_pull4h(Geo g, const S *__restrict__ src, S *__restrict__ dst,
+__global__ void __launch_bounds__(BX, 8) k_pull4h(Geo g, const S *__restrict__ src, S *__restrict__ dst,
                                                const uint8_t *__restrict__ tag,
                                                const double *__restrict__ bc, double omega,
                                                S *__restrict__ side, float sc, float inv)
@@ -412,6 +420,136 @@ __global__ void __launch_bounds__(BX) k_stream(Geo g, const S *__restrict__ src,
         const int sx = X - cx(i), sy = Y - cy(i);
         if (g.interior(sx, sy)) plane(dst, g, i)[o] = plane(src, g, i)[g.idx(sx, sy)];
         else if (in) plane(dst, g, i)[o] = side[(size_t)i * g.nper + g.pidx(X, Y)];
+    }
+}
+
+// ---- two steps per sweep (temporal blocking) ----------------------------------------------
+//
+// The GPU form of the reference's two-steps-per-sweep ("tight") idea (lb.c:442-572): a block
+// loads the collided state C_n of its TW x TH tile and a two-node halo into shared memory,
+// computes C_{n+1} on the tile and a one-node halo (the halo redundantly with the neighbouring
+// blocks: the same per-node function, so the same values), then C_{n+2} on the tile, and writes
+// only that to the other buffer.  DRAM sees one read and one write of the lattice per two
+// steps.  Each node runs pull_node's arithmetic on the same inputs, and the intermediate state
+// is kept in the storage type, so the result is identical to two single pull steps.
+//
+// Stale slots: step n+1 reads side parity (n+1)&1 (C_{n-1}); its new values go to the scratch
+// slot `side_tmp`, not to that parity, because neighbouring blocks may still read it for their
+// halo.  Step n+2 reads and writes parity n&1 for its own nodes only.  launch_pull2_finish then
+// moves the scratch into parity (n+1)&1 and swaps the two buffers' ghost rings: the state ends
+// in the buffer two single steps would not have left it in, and the read-outs take ghost values
+// from the other buffer.
+template <int TW, int TH> struct Tile2 {
+    static constexpr int W0 = TW + 4, H0 = TH + 4;    // C_n region, origin (x0 - 2, y0 - 2)
+    static constexpr int W1 = TW + 2, H1 = TH + 2;    // C_{n+1} region, origin (x0 - 1, y0 - 1)
+    static constexpr int N0 = W0 * H0, N1 = W1 * H1;
+};
+
+template <class S, int TW, int TH>
+constexpr size_t pull2_smem_bytes() { return 9 * (size_t)(Tile2<TW, TH>::N0 + Tile2<TW, TH>::N1) * sizeof(S); }
+
+constexpr int PULL2_THREADS = 256;
+
+template <class S, int TW, int TH>
+__global__ void __launch_bounds__(PULL2_THREADS) k_pull2(Geo g, const S *__restrict__ src, S *__restrict__ dst,
+                                                        const uint8_t *__restrict__ tag,
+                                                        const double *__restrict__ bc, double omega,
+                                                        const S *__restrict__ side_a, S *__restrict__ side_tmp,
+                                                        S *__restrict__ side_b, float sc, float inv)
+{
+    using T = Tile2<TW, TH>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    S *s0 = reinterpret_cast<S *>(smem_raw);          // [9][H0][W0]
+    S *s1 = s0 + 9 * T::N0;                           // [9][H1][W1]
+    const int x0 = 1 + blockIdx.x * TW, y0 = 1 + blockIdx.y * TH;
+    const int tid = threadIdx.x;
+
+    // C_n of the tile and its two-node halo (positions outside the array are never read)
+#pragma unroll 4
+    for (int k = tid; k < 9 * T::N0; k += PULL2_THREADS) {
+        const int i = k / T::N0, rc = k - i * T::N0;
+        const int r = rc / T::W0, c = rc - r * T::W0;
+        const int X = x0 - 2 + c, Y = y0 - 2 + r;
+        if (X >= 0 && X <= g.lx + 1 && Y >= 0 && Y <= g.ly + 1) s0[k] = plane(src, g, i)[g.idx(X, Y)];
+    }
+    __syncthreads();
+
+    // step n+1 on the tile and a one-node halo, into shared memory
+    for (int k = tid; k < T::N1; k += PULL2_THREADS) {
+        const int r = k / T::W1, c = k - r * T::W1;
+        const int X = x0 - 1 + c, Y = y0 - 1 + r;
+        if (!g.interior(X, Y)) continue;
+        const bool edge = g.perimeter(X, Y);
+        const int p = edge ? g.pidx(X, Y) : 0;
+        typename Work<S>::W f[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const int sx = X - cx(i), sy = Y - cy(i);
+            f[i] = Work<S>::load(g.interior(sx, sy) ? s0[i * T::N0 + (sy - y0 + 2) * T::W0 + (sx - x0 + 2)]
+                                                    : side_a[(size_t)i * g.nper + p], i, inv);
+        }
+        collide_w<S>(bc, g, tag[g.idx(X, Y)], X, Y, f, omega, sc, inv);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) s1[i * T::N1 + k] = Work<S>::store(f[i], i, sc);
+        if (edge && X >= x0 && X < x0 + TW && Y >= y0 && Y < y0 + TH) {
+#pragma unroll
+            for (int i = 0; i < 9; ++i)
+                if (!g.interior(X - cx(i), Y - cy(i))) side_tmp[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
+        }
+    }
+    __syncthreads();
+
+    // step n+2 on the tile, to the other buffer
+    for (int k = tid; k < TW * TH; k += PULL2_THREADS) {
+        const int r = k / TW, c = k - r * TW;
+        const int X = x0 + c, Y = y0 + r;
+        if (X > g.lx || Y > g.ly) continue;
+        const bool edge = g.perimeter(X, Y);
+        const int p = edge ? g.pidx(X, Y) : 0;
+        typename Work<S>::W f[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const int sx = X - cx(i), sy = Y - cy(i);
+            f[i] = Work<S>::load(g.interior(sx, sy) ? s1[i * T::N1 + (sy - y0 + 1) * T::W1 + (sx - x0 + 1)]
+                                                    : side_b[(size_t)i * g.nper + p], i, inv);
+        }
+        const long long o = g.idx(X, Y);
+        collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = Work<S>::store(f[i], i, sc);
+        if (edge) {
+#pragma unroll
+            for (int i = 0; i < 9; ++i)
+                if (!g.interior(X - cx(i), Y - cy(i))) side_b[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
+        }
+    }
+}
+
+// After k_pull2: the scratch stale slots into parity (n+1)&1, and the ghost rings of the two
+// buffers exchanged (one thread per perimeter node and per ghost-ring node).
+template <class S>
+__global__ void k_pull2_finish(Geo g, S *__restrict__ b0, S *__restrict__ b1, const S *__restrict__ side_tmp,
+                               S *__restrict__ side_a)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < g.nper) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) side_a[(size_t)i * g.nper + k] = side_tmp[(size_t)i * g.nper + k];
+    }
+    const int ng = g.nghost();
+    if (k < ng) {
+        int X, Y;
+        if (k < g.lx + 2) { X = k; Y = 0; }
+        else if (k < 2 * (g.lx + 2)) { X = k - (g.lx + 2); Y = g.ly + 1; }
+        else if (k < 2 * (g.lx + 2) + g.ly) { X = 0; Y = k - 2 * (g.lx + 2) + 1; }
+        else { X = g.lx + 1; Y = k - 2 * (g.lx + 2) - g.ly + 1; }
+        const long long o = g.idx(X, Y);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const S t = plane(b0, g, i)[o];
+            plane(b0, g, i)[o] = plane(b1, g, i)[o];
+            plane(b1, g, i)[o] = t;
+        }
     }
 }
 
@@ -933,6 +1071,11 @@ template <class S> S *SIDE(const DevLattice &d, int p)
 {
     return static_cast<S *>(d.side) + (size_t)(p & 1) * 9 * (size_t)d.g.nper;
 }
+// Pull scheme only: the scratch slot after the two parities (see k_pull2).
+template <class S> S *SIDE_TMP(const DevLattice &d)
+{
+    return static_cast<S *>(d.side) + 2 * 9 * (size_t)d.g.nper;
+}
 
 }  // namespace
 
@@ -974,6 +1117,30 @@ void launch_pull(const DevLattice &d, int src, int side_par, bool ghosts, cudaSt
         LBGPU_DISPATCH(d, (k_pull<S, false><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src),
                            d.tag, d.bc, d.omega, SIDE<S>(d, side_par), d.scale, d.inv_scale)));
     }
+}
+
+template <class S, int TW, int TH>
+static void launch_pull2_t(const DevLattice &d, int src, int n_par, cudaStream_t s)
+{
+    constexpr size_t smem = pull2_smem_bytes<S, TW, TH>();
+    cudaFuncSetAttribute(k_pull2<S, TW, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 grid(cdiv(d.g.lx, TW), cdiv(d.g.ly, TH));
+    k_pull2<S, TW, TH><<<grid, PULL2_THREADS, smem, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
+                                                      SIDE<S>(d, n_par + 1), SIDE_TMP<S>(d), SIDE<S>(d, n_par),
+                                                      d.scale, d.inv_scale);
+}
+
+void launch_pull2(const DevLattice &d, int src, int n_par, cudaStream_t s)
+{
+    switch (d.precision) {
+    case LBGPU_F64: launch_pull2_t<double, 32, 16>(d, src, n_par, s); break;
+    case LBGPU_F32: launch_pull2_t<float, 64, 16>(d, src, n_par, s); break;
+    case LBGPU_F16: launch_pull2_t<__half, 64, 16>(d, src, n_par, s); break;
+    default: launch_pull2_t<__nv_bfloat16, 64, 16>(d, src, n_par, s); break;
+    }
+    const int nthreads = std::max(d.g.nper, d.g.nghost());
+    LBGPU_DISPATCH(d, (k_pull2_finish<S><<<cdiv(nthreads, 256), 256, 0, s>>>(d.g, B<S>(d, 0), B<S>(d, 1),
+                       SIDE_TMP<S>(d), SIDE<S>(d, n_par + 1))));
 }
 
 void launch_stream(const DevLattice &d, int src, int side_par, cudaStream_t s)

@@ -11,7 +11,7 @@ struct DevLattice {
     Geo g;
     int precision;       // LBGPU_F64 / F32 / F16 / BF16: element type of buf and side
     void *buf[2];        // population buffers (buf[1] unused by the AA scheme)
-    void *side;          // stale-slot store [2][9][nper]
+    void *side;          // stale-slot store [2][9][nper] (+ a scratch [9][nper] for pull lattices)
     void *ghost2;        // AA only: the second buffer's ghost ring [9][nghost] (see logical())
     const uint8_t *tag;  // tag plane
     double *bc;          // boundary tables [8][2][nb]
@@ -31,6 +31,10 @@ enum { VIEW_DIRECT = 0, VIEW_PULL_PENDING = 1, VIEW_AA_NATURAL = 2, VIEW_AA_SWAP
 void launch_collide_inplace(const DevLattice &d, int cur, int side_par, cudaStream_t s);
 void launch_pull(const DevLattice &d, int src, int side_par, bool ghosts, cudaStream_t s);
 void launch_stream(const DevLattice &d, int src, int side_par, cudaStream_t s);
+// Two pull steps in one sweep (temporal blocking): C_n in buffer src (n_par = n & 1) ->
+// C_{n+2} in buffer 1 - src, then the stale-slot scratch into parity n+1 and the two buffers'
+// ghost rings exchanged.  Pull lattices without ghost-ring output only.
+void launch_pull2(const DevLattice &d, int src, int n_par, cudaStream_t s);
 void launch_side_from_buf(const DevLattice &d, int b, int side_par, cudaStream_t s);
 // AA only: keep buffer b's ghost ring as the second buffer's (d.ghost2).
 void launch_ghost_copy(const DevLattice &d, int b, cudaStream_t s);

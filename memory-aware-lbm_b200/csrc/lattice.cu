@@ -79,7 +79,8 @@ int Lattice::create(int lx_, int ly_, int precision_, int scheme_)
 
     const size_t nbuf = (scheme == LBGPU_AA) ? 1 : 2;
     const size_t pbytes = 9 * (size_t)d.g.plane * elem;
-    const size_t sbytes = 2 * 9 * (size_t)d.g.nper * elem;
+    // two parities, and for the pull scheme the scratch of the two-step kernel
+    const size_t sbytes = (scheme == LBGPU_PULL ? 3 : 2) * 9 * (size_t)d.g.nper * elem;
     void *p = nullptr;
     for (size_t b = 0; b < nbuf; ++b) {
         LB_CUDA(cudaMalloc(&p, pbytes), "cudaMalloc(populations)");
@@ -238,6 +239,14 @@ int Lattice::step(int nsteps)
         if (zgb_each_step) LB_TRY(zgb_pass());
         if (scheme == LBGPU_AA) {
             LB_TRY(aa_step());
+        } else if (sweep_steps == 2 && nsteps - s >= 2 && !zgb_each_step && !ghosts && form == FORM_C && pending) {
+            // two steps in one sweep: C_n -> C_{n+2} in the other buffer, still pending
+            launch_pull2(d, cur, (int)(n & 1), stream);
+            launches += 2;
+            cur = 1 - cur;
+            n += 2;
+            ++s;
+            LB_TRY(check("two-step pull"));
         } else {
             LB_TRY(op_collide());
             LB_TRY(op_propagate());

@@ -203,6 +203,16 @@ int lbgpu_setup_cylinder(lbgpu_lattice *h, int obst_x, int obst_y, int obst_r, d
     return lbgpu::cuda_error(cudaStreamSynchronize(L.stream), "lbgpu_setup_cylinder");
 }
 
+int lbgpu_set_sweep_steps(lbgpu_lattice *h, int steps)
+{
+    if (int rc = bad_handle(h, "lbgpu_set_sweep_steps")) return rc;
+    if (steps != 1 && steps != 2) return set_error(LB_ERR_ARG, "lbgpu_set_sweep_steps: %d (1 or 2)", steps);
+    if (steps == 2 && h->L.scheme != LBGPU_PULL)
+        return set_error(LB_ERR_STATE, "two steps per sweep needs the pull scheme");
+    h->L.sweep_steps = steps;
+    return LB_OK;
+}
+
 int lbgpu_step(lbgpu_lattice *h, int nsteps)
 {
     if (int rc = bad_handle(h, "lbgpu_step")) return rc;

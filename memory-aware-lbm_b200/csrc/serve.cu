@@ -133,7 +133,8 @@ size_t lbgpu_lattice_bytes(int lx, int ly, int precision, int scheme)
     const int elem = precision == LBGPU_F64 ? 8 : (precision == LBGPU_F32 ? 4 : 2);
     const lbgpu::Geo g = lbgpu::make_geo(lx, ly, elem);
     const size_t nbuf = scheme == LBGPU_AA ? 1 : 2;
-    size_t b = nbuf * 9 * (size_t)g.plane * elem + 2 * 9 * (size_t)g.nper * elem + (size_t)g.plane +
+    const size_t nside = scheme == LBGPU_AA ? 2 : 3;
+    size_t b = nbuf * 9 * (size_t)g.plane * elem + nside * 9 * (size_t)g.nper * elem + (size_t)g.plane +
                16 * (size_t)g.nb * 8 + 4 * (size_t)g.nb * 4 + 2 * (size_t)(ly + 2) * 8;
     if (scheme == LBGPU_AA) b += 9 * (size_t)g.nghost() * elem;
     return b;

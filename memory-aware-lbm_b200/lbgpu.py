@@ -88,6 +88,7 @@ def lib():
     L.lbgpu_build_cylinder.argtypes = [ctypes.c_int] * 5 + [ctypes.c_double] * 2 + [
         ctypes.c_int] * 2 + [_u8p, _dp, _u8p, _dp]
     L.lbgpu_step.argtypes = [_vp, ctypes.c_int]
+    L.lbgpu_set_sweep_steps.argtypes = [_vp, ctypes.c_int]
     L.lbgpu_step_timed.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     L.lbgpu_get_populations.argtypes = [_vp, _dp]
     L.lbgpu_get_macros.argtypes = [_vp, _dp, _dp, _dp]
@@ -231,6 +232,10 @@ class Lattice:
         _check(lib().lbgpu_setup_cylinder(self.h, obst_x, obst_y, obst_r, umax, re, wall, outlet,
                                           ctypes.byref(om)))
         return om.value
+
+    def set_sweep_steps(self, steps):
+        """1, or 2 for two pull steps per sweep (temporal blocking)."""
+        _check(lib().lbgpu_set_sweep_steps(self.h, int(steps)))
 
     def step(self, n):
         _check(lib().lbgpu_step(self.h, int(n)))

@@ -73,19 +73,23 @@ def tune_schemes(precision, sizes, steps=6):
     return out
 
 
-def batching_study(precisions=("f32", "f16"), n=512, steps=2000, seed=20260101):
+def batching_study(precisions=("f32", "f16"), n=512, steps=2000, seed=20260101, tune=1):
+    """tune=0 keeps the defaults (pull members, default tile shapes and launch form)."""
     insts = batching_instances(n, seed)
     nodes = sum(q["lx"] * q["ly"] for q in insts)
     res = {"instances": n, "seed": seed, "nodes": nodes, "steps": steps, "chunk": 50,
            "precisions": {}}
     for prec in precisions:
-        schemes = tune_schemes(prec, [(q["lx"], q["ly"]) for q in insts])
+        if tune:
+            schemes = tune_schemes(prec, [(q["lx"], q["ly"]) for q in insts])
+        else:
+            schemes = {lbgpu.size_class(q["lx"] * q["ly"]): {"scheme": "pull"} for q in insts}
         lats = [_channel(q, prec, schemes[lbgpu.size_class(q["lx"] * q["ly"])]["scheme"])
                 for q in insts]
         try:
             with lbgpu.Batch(prec) as b:
                 slots = [b.add(l) for l in lats]
-                best = b.autotune(4)
+                best = b.autotune(4) if tune else [0.0] * 6
                 shapes = {c: list(b.shape(c)) for c in schemes}
                 persistent = b.persistent
                 threads = b.threads
