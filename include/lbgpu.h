@@ -247,6 +247,7 @@ typedef struct {
     long long steps, nodes;
     int converged, done;            /* converged: 1 steady, 0 step cap, -1 diverged */
     double last_change;             /* velocity change over the last check interval */
+    int solo;                       /* 1: stepped on its own, not as a batch member */
 } lbgpu_result;
 
 typedef struct lbgpu_server lbgpu_server;
@@ -256,6 +257,10 @@ int lbgpu_server_set_scheme(lbgpu_server *s, int size_class, int scheme);
 int lbgpu_server_set_shape(lbgpu_server *s, int size_class, int tile_width, int nodes_per_thread);
 int lbgpu_server_set_persistent(lbgpu_server *s, int persistent);
 int lbgpu_server_set_threads(lbgpu_server *s, int threads);
+/* Requests of at least `nodes` lattice nodes (default 2^20) are not batch members: they fill
+ * the GPU on their own and step with the single-lattice kernels on their own streams,
+ * concurrently with the batch; 0 batches every request. */
+int lbgpu_server_set_solo_nodes(lbgpu_server *s, long long nodes);
 int lbgpu_server_set_offset_scale(lbgpu_server *s, int scale_log2);
 int lbgpu_server_submit(lbgpu_server *s, const lbgpu_request *r, int *id);
 int lbgpu_server_run(lbgpu_server *s, int batched);

@@ -2,11 +2,13 @@
 //
 // Requests (a cylinder channel, a step cap and a steady-state tolerance) arrive over wall-clock
 // time.  The loop admits them in arrival order while their lattices fit the HBM budget, keeps
-// every admitted lattice resident as a member of one batch (one persistent launch per step for
-// all of them), advances the batch `check_every` steps at a time, and after each advance
+// every admitted lattice resident, advances them `check_every` steps at a time, and after each advance
 // retires every member that reached its step cap or whose largest velocity change over those
 // steps fell below its tolerance (device reduction, one copy back for all members).  Retiring
-// frees the member's memory, which admits waiting requests at the next round.
+// frees the member's memory, which admits waiting requests at the next round.  Lattices below
+// the solo size are members of one batch (one launch per step for all of them); larger ones,
+// which fill the GPU on their own, step with the single-lattice kernels on their own streams,
+// concurrently with the batch.
 //
 // The sequential mode serves the same requests one at a time, each stepped on its own
 // (plain solves: the single-lattice kernels, no batch, no graphs), as the comparison.
@@ -33,6 +35,7 @@ struct Req {
     int converged = 0;
     float change = -1.0f;
     bool active = false, done = false;
+    bool solo = false;           // stepped on its own stream instead of in the batch
     std::vector<double> ux, uy;
 };
 
@@ -54,6 +57,7 @@ struct lbgpu_server {
     int shape_n[6] = {1, 1, 1, 1, 1, 1};     // and nodes per thread
     int persistent = -1;                     // batch launch form, -1 = default
     int threads = 0;                         // batch threads per tile, 0 = default
+    long long solo_nodes = 1LL << 20;        // requests of this many nodes or more step on their own
     size_t budget = 0;
     int check_every = 100;
     int scale_log2 = 10;
@@ -202,6 +206,13 @@ int lbgpu_server_set_threads(lbgpu_server *s, int threads)
     return LB_OK;
 }
 
+int lbgpu_server_set_solo_nodes(lbgpu_server *s, long long nodes)
+{
+    if (!s || nodes < 0) return set_error(LB_ERR_ARG, "lbgpu_server_set_solo_nodes: bad arguments");
+    s->solo_nodes = nodes;
+    return LB_OK;
+}
+
 int lbgpu_server_set_offset_scale(lbgpu_server *s, int scale_log2)
 {
     if (!s || scale_log2 < -30 || scale_log2 > 30) return set_error(LB_ERR_ARG, "lbgpu_server_set_offset_scale");
@@ -261,7 +272,8 @@ int lbgpu_server_run(lbgpu_server *s, int batched)
             if ((rc = start(s, q))) break;
             q.admit = now_s(t0);
             used += need;
-            if (batched && (rc = lbgpu_batch_add(batch, q.lat, &q.slot))) break;
+            q.solo = batched && (long long)q.spec.lx * q.spec.ly >= s->solo_nodes && s->solo_nodes > 0;
+            if (batched && !q.solo && (rc = lbgpu_batch_add(batch, q.lat, &q.slot))) break;
             active.push_back(order[qi]);
             ++qi;
         }
@@ -276,6 +288,9 @@ int lbgpu_server_run(lbgpu_server *s, int batched)
         // advance every active request by check_every steps
         if (batched) {
             if ((rc = lbgpu_batch_step(batch, s->check_every))) break;
+            for (int i : active)
+                if (s->reqs[i].solo && (rc = lbgpu_step(s->reqs[i].lat, s->check_every))) break;
+            if (rc) break;
         } else {
             if ((rc = lbgpu_step(s->reqs[active[0]].lat, s->check_every))) break;
         }
@@ -310,7 +325,7 @@ int lbgpu_server_run(lbgpu_server *s, int batched)
                     q.uy.resize((size_t)q.spec.lx * q.spec.ly);
                     if ((rc = lbgpu_get_macros(q.lat, nullptr, q.ux.data(), q.uy.data()))) break;
                 }
-                if (batched && (rc = lbgpu_batch_remove(batch, q.slot))) break;
+                if (batched && !q.solo && (rc = lbgpu_batch_remove(batch, q.slot))) break;
                 q.finish = now_s(t0);
                 used -= q.bytes;
                 release(q);
@@ -339,6 +354,7 @@ int lbgpu_server_result(lbgpu_server *s, int id, lbgpu_result *out, double *ux, 
     out->last_change = q.change;
     out->nodes = (long long)q.spec.lx * q.spec.ly;
     out->done = q.done ? 1 : 0;
+    out->solo = q.solo ? 1 : 0;
     if (ux && !q.ux.empty()) std::memcpy(ux, q.ux.data(), q.ux.size() * sizeof(double));
     if (uy && !q.uy.empty()) std::memcpy(uy, q.uy.data(), q.uy.size() * sizeof(double));
     return LB_OK;

@@ -57,7 +57,7 @@ class Result(ctypes.Structure):
     _fields_ = [("arrival", ctypes.c_double), ("admit", ctypes.c_double),
                 ("finish", ctypes.c_double), ("steps", ctypes.c_longlong),
                 ("nodes", ctypes.c_longlong), ("converged", ctypes.c_int),
-                ("done", ctypes.c_int), ("last_change", ctypes.c_double)]
+                ("done", ctypes.c_int), ("last_change", ctypes.c_double), ("solo", ctypes.c_int)]
 
 
 _LIB = None
@@ -128,6 +128,7 @@ def lib():
     L.lbgpu_server_set_shape.argtypes = [_vp] + [ctypes.c_int] * 3
     L.lbgpu_server_set_persistent.argtypes = [_vp, ctypes.c_int]
     L.lbgpu_server_set_threads.argtypes = [_vp, ctypes.c_int]
+    L.lbgpu_server_set_solo_nodes.argtypes = [_vp, ctypes.c_longlong]
     L.lbgpu_server_set_offset_scale.argtypes = [_vp, ctypes.c_int]
     L.lbgpu_server_submit.argtypes = [_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int)]
     L.lbgpu_server_run.argtypes = [_vp, ctypes.c_int]
@@ -491,6 +492,10 @@ class Server:
 
     def set_threads(self, n):
         _check(lib().lbgpu_server_set_threads(self.h, int(n)))
+
+    def set_solo_nodes(self, nodes):
+        """Requests of at least this many nodes step on their own (0: batch every request)."""
+        _check(lib().lbgpu_server_set_solo_nodes(self.h, int(nodes)))
 
     def submit(self, lx, ly, obst_x, obst_y, obst_r, umax, re, max_steps, tol=0.0, arrival=0.0,
                want_fields=False):

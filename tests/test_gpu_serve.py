@@ -32,8 +32,10 @@ def requests(seed, n):
     return out
 
 
-def serve(precision, reqs, batched, budget):
+def serve(precision, reqs, batched, budget, solo_nodes=None):
     with lbgpu.Server(precision, budget, CHECK) as srv:
+        if solo_nodes is not None:
+            srv.set_solo_nodes(solo_nodes)
         ids = [srv.submit(**q) for q in reqs]
         srv.run(batched)
         res = [srv.result(i, fields=True) for i in ids]
@@ -51,12 +53,20 @@ def alone(precision, q, steps):
         return ux, uy
 
 
-@pytest.mark.parametrize("precision", ["f32", "f16", "f64"])
-def test_served_results_match_sequential_and_alone(precision):
+@pytest.mark.parametrize("precision,solo_nodes", [("f32", 0), ("f16", 0), ("f64", 0),
+                                                 ("f32", 12000), ("f16", 12000)])
+def test_served_results_match_sequential_and_alone(precision, solo_nodes):
+    """solo_nodes 0: every request a batch member; 12000: the larger ones step on their own."""
     reqs = requests(7, 12)
     budget = sum(lbgpu.lattice_bytes(q["lx"], q["ly"], precision) + 8 * q["lx"] * q["ly"]
                  for q in reqs) // 3       # about a third of the requests fit at once
-    mix, st_mix = serve(precision, reqs, True, budget)
+    mix, st_mix = serve(precision, reqs, True, budget, solo_nodes)
+    solo = [r["solo"] for r in mix]
+    if solo_nodes:
+        assert any(solo) and not all(solo)
+        assert solo == [int(q["lx"] * q["ly"] >= solo_nodes) for q in reqs]
+    else:
+        assert not any(solo)
     seq, st_seq = serve(precision, reqs, False, budget)
     assert st_mix["peak_bytes"] <= budget and st_seq["peak_bytes"] <= budget
     assert st_mix["peak_resident"] > 1 and st_seq["peak_resident"] == 1
