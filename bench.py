@@ -385,7 +385,7 @@ def run_ours(args, dist):
         "metric": "MLUPS", "value": round(mlups, 1), "unit": "MLUPS", "n_gpus": dist.world,
         "steps": K, "warmup": W, "ms_per_step": round(ms / K, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
-        "config": {"workload": f"cylinder channel {nx}x{ny} (67.1M nodes), Re=100, uMax=0.02, "
+        "config": {"workload": f"cylinder channel {nx}x{ny} ({nodes / 1e6:.1f}M nodes), Re=100, uMax=0.02, "
                                f"{args.precision.upper()} {args.scheme} kernel",
                    "nodes_per_gpu": nodes, "l2": "inputs larger than L2 (lattice "
                    f"{bpu * nodes / 1e9:.1f} GB streamed per step)",
