@@ -41,7 +41,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "memory-aware-lbm_b200")
 sys.path.insert(0, PKG)
 
-BYTES_PER_UPDATE = {"f64": 144, "f32": 72, "f16": 36, "bf16": 36}
+BYTES_PER_UPDATE = {"f64": 144, "f32": 72, "f16": 36, "bf16": 36,
+                    "f16s": 36, "bf16s": 36}   # "s": 16-bit offsets from the inflow profile per row
 
 
 def parse():
@@ -281,12 +282,16 @@ def run_reference_arm(args, dist):
 # ---------------------------------------------------------------------------------------
 def time_lattice(lbgpu, nx, ny, precision, scheme, steps, warmup, dist, sampler_dev=None):
     ox, oy, r = cylinder(nx, ny)
-    lat = lbgpu.Lattice(nx, ny, precision, "pull" if scheme == "pull2" else scheme)
+    shifted = precision.endswith("s")
+    base = precision[:-1] if shifted else precision
+    lat = lbgpu.Lattice(nx, ny, base, "pull" if scheme == "pull2" else scheme)
     try:
         if scheme == "pull2":
             lat.set_sweep_steps(2)
-        if precision in ("f16", "bf16"):   # the scale encodes the initial state: set it first
-            lat.set_offset_scale(lbgpu_default_scale(precision))
+        if base in ("f16", "bf16"):   # the scale and shift encode the initial state: set them first
+            lat.set_offset_scale((lbgpu.DEFAULT_SHIFT_SCALE if shifted else lbgpu.DEFAULT_SCALE)[base])
+        if shifted:
+            lat.set_offset_shift(lbgpu.poiseuille_profile(ny, 0.02))
         lat.setup_cylinder(ox, oy, r, 0.02, 100.0, lbgpu.WALL_BOUNCEBACK, lbgpu.OUTLET_CONST)
         lat.step(warmup)
         lat.synchronize()
@@ -304,10 +309,6 @@ def time_lattice(lbgpu, nx, ny, precision, scheme, steps, warmup, dist, sampler_
         return ms, launches, clocks
     finally:
         lat.close()
-
-
-def lbgpu_default_scale(precision):
-    return 10 if precision == "f16" else 6
 
 
 def run_ours(args, dist):

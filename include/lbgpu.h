@@ -117,6 +117,17 @@ int lbgpu_set_populations(lbgpu_lattice *lat, const double *f, const double *tmp
 /* Power-of-two scale s of the FP16/BF16 offset storage: stored = (f_i - w_i) * 2^s. */
 int lbgpu_set_offset_scale(lbgpu_lattice *lat, int scale_log2);
 
+/* FP16/BF16 storage only: store offsets from the equilibrium of a per-row shift velocity
+ * instead of from the lattice weights: stored_i = (f_i - f_eq_i(1, (u_row[Y], 0))) * 2^s, where
+ * Y is the row that consumes the value (the receiving row after streaming).  For a channel whose
+ * flow stays close to a known profile (the Poiseuille inflow of lbgpu_setup_cylinder, 4 uMax
+ * (L y - y^2) / L^2 with y = Y - 1, L = ly - 1, and 0 in the ghost rows), the stored values are
+ * small deviations, which the 16-bit significand resolves far better than offsets from w_i; it
+ * removes the slow drift of the smooth far field.  u_row has ly + 2 values (|u| < 0.5); NULL
+ * returns to offsets from w_i.  Set it, like the scale, before the initial state is written.
+ * LB_ERR_STATE for FP64/FP32 lattices.  No counterpart in the reference (FP64 only). */
+int lbgpu_set_offset_shift(lbgpu_lattice *lat, const double *u_row);
+
 /* Cylinder channel on the device without host population arrays: tags and tables as the
  * application driver builds them (obstacle disk, walls, Poiseuille inlet, pressure outlet)
  * and equilibrium populations at rho = 1 and the Poiseuille profile.  Returns omega through
@@ -262,6 +273,9 @@ int lbgpu_server_set_threads(lbgpu_server *s, int threads);
  * concurrently with the batch; 0 batches every request. */
 int lbgpu_server_set_solo_nodes(lbgpu_server *s, long long nodes);
 int lbgpu_server_set_offset_scale(lbgpu_server *s, int scale_log2);
+/* FP16/BF16 servers: store each request's offsets from its inflow profile's equilibrium per
+ * row (lbgpu_set_offset_shift) instead of from w_i. */
+int lbgpu_server_set_offset_shift(lbgpu_server *s, int on);
 int lbgpu_server_submit(lbgpu_server *s, const lbgpu_request *r, int *id);
 int lbgpu_server_run(lbgpu_server *s, int batched);
 int lbgpu_server_result(lbgpu_server *s, int id, lbgpu_result *out, double *ux, double *uy);

@@ -36,16 +36,22 @@ __device__ __forceinline__ S *plane(S *b, const Geo &g, int i)
 }
 
 // Table entry (p0, p1) of a boundary node: (ux, uy) or (rho, uPar).
-__device__ __forceinline__ void node_params(const double *__restrict__ bc, const Geo &g, int t,
-                                            int X, int Y, double &p0, double &p1)
+__device__ __forceinline__ void node_params(const double *__restrict__ bc, int nb, int t, int X, int Y,
+                                            double &p0, double &p1)
 {
     p0 = 0.0; p1 = 0.0;
     if (t >= TAG_ZOUHE_FIRST && t < TAG_COUNT) {
         const int tb = tag_table(t);
         const int coord = (tag_side(t) <= SIDE_LOWER) ? X : Y;
-        p0 = bc[(tb * 2 + 0) * g.nb + coord];
-        p1 = bc[(tb * 2 + 1) * g.nb + coord];
+        p0 = bc[(tb * 2 + 0) * nb + coord];
+        p1 = bc[(tb * 2 + 1) * nb + coord];
     }
+}
+
+__device__ __forceinline__ void node_params(const double *__restrict__ bc, const Geo &g, int t,
+                                            int X, int Y, double &p0, double &p1)
+{
+    node_params(bc, g.nb, t, X, Y, p0, p1);
 }
 
 template <class S>
@@ -57,6 +63,9 @@ __device__ __forceinline__ void collide_node(const double *__restrict__ bc, cons
     node_params(bc, g, t, X, Y, p0, p1);
     rules::collide<R>(t, f, (R)omega, (R)p0, (R)p1);
 }
+
+template <class S>
+__device__ __forceinline__ typename Codec<S>::R dec_row(const Geo &g, S v, int i, float inv, int Y);
 
 // Post-stream value of slot i at node (X, Y), any node of the lattice including the ghost
 // ring, under each view (kernels.h).  Ghost slots that no interior node streams into keep the
@@ -74,19 +83,19 @@ __device__ __forceinline__ typename Codec<S>::R logical(const Geo &g, int view, 
     const int sx = X - cx(i), sy = Y - cy(i);
     switch (view) {
     case VIEW_PULL_PENDING:
-        if (g.interior(sx, sy)) return C::dec(plane(cur, g, i)[g.idx(sx, sy)], i, inv);
-        if (g.interior(X, Y)) return C::dec(side[(size_t)i * g.nper + g.pidx(X, Y)], i, inv);
-        return C::dec(plane(other, g, i)[g.idx(X, Y)], i, inv);
+        if (g.interior(sx, sy)) return dec_row<S>(g, plane(cur, g, i)[g.idx(sx, sy)], i, inv, Y);
+        if (g.interior(X, Y)) return dec_row<S>(g, side[(size_t)i * g.nper + g.pidx(X, Y)], i, inv, Y);
+        return dec_row<S>(g, plane(other, g, i)[g.idx(X, Y)], i, inv, Y);
     case VIEW_AA_NATURAL:
         if (g.interior(X, Y) && !g.interior(sx, sy))
-            return C::dec(side[(size_t)i * g.nper + g.pidx(X, Y)], i, inv);
-        return C::dec(plane(cur, g, i)[g.idx(X, Y)], i, inv);
+            return dec_row<S>(g, side[(size_t)i * g.nper + g.pidx(X, Y)], i, inv, Y);
+        return dec_row<S>(g, plane(cur, g, i)[g.idx(X, Y)], i, inv, Y);
     case VIEW_AA_SWAPPED:
-        if (g.interior(sx, sy)) return C::dec(plane(cur, g, opp(i))[g.idx(sx, sy)], i, inv);
-        if (g.interior(X, Y)) return C::dec(side[(size_t)i * g.nper + g.pidx(X, Y)], i, inv);
-        return C::dec(other[(size_t)i * g.nghost() + g.gidx(X, Y)], i, inv);
+        if (g.interior(sx, sy)) return dec_row<S>(g, plane(cur, g, opp(i))[g.idx(sx, sy)], i, inv, Y);
+        if (g.interior(X, Y)) return dec_row<S>(g, side[(size_t)i * g.nper + g.pidx(X, Y)], i, inv, Y);
+        return dec_row<S>(g, other[(size_t)i * g.nghost() + g.gidx(X, Y)], i, inv, Y);
     default:
-        return C::dec(plane(cur, g, i)[g.idx(X, Y)], i, inv);
+        return dec_row<S>(g, plane(cur, g, i)[g.idx(X, Y)], i, inv, Y);
     }
 }
 
@@ -124,35 +133,52 @@ template <> struct Half2Ops<__nv_bfloat16> {
 // and the relaxation is D_i' = (1 - omega) D_i + omega E_i.  Opposite directions i, opp(i)
 // share c.u and c.j up to sign: omega E_i, omega E_opp = a +- b with
 // a = k (A + 4.5 (c.u)(c.j)), b = 3 k c.j, k = omega sc w.
+// With a row shift (SHIFT, offsets relative to S_i = f_eq_i(1, (us, 0)) instead of w_i):
+// j = (us, 0) + inv J, E_i = sc (f_eq_i(rho, u) - S_i), so A gains -1.5 us (ux - us) and a gains
+// 4.5 k (c.us)(c.u - c.us); b is unchanged.  Without it the arithmetic is exactly the unshifted one.
 // 1/rho uses the hardware reciprocal (the 16-bit path is held to a tolerance, not bit-exact).
-__device__ __forceinline__ void bgk_offsets(float D[9], float omega, float sc, float inv)
+template <bool SHIFT>
+__device__ __forceinline__ void bgk_offsets(float D[9], float omega, float sc, float inv, float us)
 {
-    // J = 2^s j (scaled sums): u = J inv / rho, and inv folds into the constants below
+    // J = 2^s (j - us): scaled sums; u = J inv / rho (+ us / rho), inv folded into constants
     const float sum = ((D[0] + D[1]) + (D[2] + D[3])) + ((D[4] + D[5]) + (D[6] + D[7])) + D[8];
     const float d = inv * sum;
     const float Jx = (D[1] - D[3]) + (D[5] - D[6]) + (D[8] - D[7]);
     const float Jy = (D[2] - D[4]) + (D[5] - D[8]) + (D[6] - D[7]);
-    const float q = inv * __fdividef(1.0f, 1.0f + d);
-    const float ux = Jx * q, uy = Jy * q;
-    const float A = fmaf(-1.5f * inv, fmaf(Jx, ux, Jy * uy), d);
+    const float ir = __fdividef(1.0f, 1.0f + d);
+    const float q = inv * ir;
+    const float ux = SHIFT ? fmaf(Jx, q, __fmul_rn(us, ir)) : Jx * q, uy = Jy * q;
+    float A = fmaf(-1.5f * inv, fmaf(Jx, ux, Jy * uy), d);
+    if (SHIFT) A = fmaf(-1.5f * us, __fsub_rn(ux, us), A);
     const float ux45 = (4.5f * inv) * ux, uy45 = (4.5f * inv) * uy;
+    const float hs = 4.5f * us;
     const float om1 = 1.0f - omega;
     const float k0 = omega * sc * (4.f / 9.f), k1 = omega * sc * (1.f / 9.f), k2 = omega * sc * (1.f / 36.f);
     D[0] = fmaf(om1, D[0], k0 * A);
-#define LBGPU_PAIR(I, J, K, CU45, CJ)                                  \
+    // The shifted terms use explicitly rounded operations: no multiply-add contraction may
+    // differ between the kernels that inline this, so every scheme stays bit-identical.
+#define LBGPU_PAIR(I, J, K, CU45, CJ, EXTRA)                           \
     {                                                                  \
         const float cj = (CJ);                                         \
-        const float a = K * fmaf(CU45, cj, A);                         \
-        const float b = ((3.0f * inv) * K) * cj;                       \
-        D[I] = fmaf(om1, D[I], a + b);                                 \
-        D[J] = fmaf(om1, D[J], a - b);                                 \
+        if (SHIFT) {                                                   \
+            const float a = __fmul_rn(K, __fadd_rn(fmaf(CU45, cj, A), (EXTRA))); \
+            const float b = __fmul_rn((3.0f * inv) * K, cj);          \
+            D[I] = fmaf(om1, D[I], __fadd_rn(a, b));                   \
+            D[J] = fmaf(om1, D[J], __fsub_rn(a, b));                   \
+        } else {                                                       \
+            const float a = K * fmaf(CU45, cj, A);                     \
+            const float b = ((3.0f * inv) * K) * cj;                   \
+            D[I] = fmaf(om1, D[I], a + b);                             \
+            D[J] = fmaf(om1, D[J], a - b);                             \
+        }                                                              \
     }
-    LBGPU_PAIR(1, 3, k1, ux45, Jx)
-    LBGPU_PAIR(2, 4, k1, uy45, Jy)
-    LBGPU_PAIR(5, 7, k2, ux45 + uy45, Jx + Jy)
-    LBGPU_PAIR(6, 8, k2, uy45 - ux45, Jy - Jx)
+    LBGPU_PAIR(1, 3, k1, ux45, Jx, __fmul_rn(hs, __fsub_rn(ux, us)))
+    LBGPU_PAIR(2, 4, k1, uy45, Jy, 0.0f)
+    LBGPU_PAIR(5, 7, k2, __fadd_rn(ux45, uy45), __fadd_rn(Jx, Jy), __fmul_rn(hs, __fsub_rn(__fadd_rn(ux, uy), us)))
+    LBGPU_PAIR(6, 8, k2, __fsub_rn(uy45, ux45), __fsub_rn(Jy, Jx), __fmul_rn(-hs, __fadd_rn(__fsub_rn(uy, ux), us)))
 #undef LBGPU_PAIR
 }
+
 
 // Working values of a kernel: decoded populations f for FP64/FP32, the stored offsets D as
 // float for 16-bit storage (see bgk_offsets); collide_w applies a node's rule to them.  Every
@@ -173,8 +199,43 @@ template <> struct Work<__nv_bfloat16> {
     static __device__ __forceinline__ __nv_bfloat16 store(float w, int, float) { return __float2bfloat16_rn(w); }
 };
 
+// Decode / encode of a value consumed at row Y (read-outs, uploads, initial states).
+template <class S>
+__device__ __forceinline__ typename Codec<S>::R dec_row(const Geo &g, S v, int i, float inv, int Y)
+{
+    if constexpr (sizeof(S) == 2) {
+        if (g.shift_u) return fmaf(Work<S>::load(v, i, inv), inv, g.shift_base(Y)[i]);
+    }
+    return Codec<S>::dec(v, i, inv);
+}
+
+template <class S>
+__device__ __forceinline__ S enc_row(const Geo &g, typename Codec<S>::R f, int i, float sc, int Y)
+{
+    if constexpr (sizeof(S) == 2) {
+        if (g.shift_u) return Work<S>::store(__fmul_rn(__fsub_rn(f, g.shift_base(Y)[i]), sc), i, sc);
+    }
+    return Codec<S>::enc(f, i, sc);
+}
+
+// A post-collision value of direction i at row Y, as stored in a population plane: with a row
+// shift it is relative to the row that consumes it after streaming, Y + c_iy (stale-slot copies
+// in the side store are consumed by the node itself and stay relative to row Y).
+// SH: 0 no shift, 1 shift (known at compile time), 2 decided by g.shift_u at run time.
+template <class S, int SH = 2>
+__device__ __forceinline__ typename Work<S>::W stored_out(const Geo &g, int Y, int i, typename Work<S>::W w,
+                                                          float sc)
+{
+    if constexpr (sizeof(S) == 2 && SH != 0) {
+        if (cy(i) != 0 && (SH == 1 || g.shift_u))
+            return __fadd_rn(w, __fmul_rn(g.shift_rebase(Y)[i], sc));
+    }
+    return w;
+}
+
 // A non-BGK rule on one node's 16-bit offsets: decode, the generic rule, encode.  Out of line so
-// the bulk path keeps its registers (it runs for boundary and obstacle nodes only).
+// the bulk path keeps its registers (it runs for boundary and obstacle nodes only); the shifted
+// form is a separate function, because a larger callee costs the 64-register quad kernel spills.
 template <class S>
 static __device__ __noinline__ void boundary_offsets(const double *__restrict__ bc, Geo g, int t, int X,
                                                      int Y, float D[9], double omega, float sc, float inv)
@@ -187,19 +248,41 @@ static __device__ __noinline__ void boundary_offsets(const double *__restrict__ 
     for (int i = 0; i < 9; ++i) D[i] = (f[i] - wgtf(i)) * sc;
 }
 
+// The same with offsets from the row's shift equilibrium (base: S_i of the row).
 template <class S>
+static __device__ __noinline__ void boundary_offsets_shifted(const double *__restrict__ bc, int nb,
+                                                             const float *__restrict__ base, int t, int X, int Y,
+                                                             float D[9], double omega, float sc, float inv)
+{
+    float f[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) f[i] = fmaf(D[i], inv, base[i]);
+    double p0, p1;
+    node_params(bc, nb, t, X, Y, p0, p1);
+    rules::collide<float>(t, f, (float)omega, (float)p0, (float)p1);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) D[i] = (f[i] - base[i]) * sc;
+}
+
+template <class S, int SH = 2>
 __device__ __forceinline__ void collide_w(const double *__restrict__ bc, const Geo &g, int t, int X,
                                           int Y, typename Work<S>::W w[9], double omega, float sc,
                                           float inv)
 {
     if constexpr (sizeof(S) == 2) {
         if (t == TAG_BGK) {
-            bgk_offsets(w, (float)omega, sc, inv);
+            if constexpr (SH == 1) bgk_offsets<true>(w, (float)omega, sc, inv, g.shift_u[Y]);
+            else if constexpr (SH == 0) bgk_offsets<false>(w, (float)omega, sc, inv, 0.0f);
+            else if (g.shift_u) bgk_offsets<true>(w, (float)omega, sc, inv, g.shift_u[Y]);
+            else bgk_offsets<false>(w, (float)omega, sc, inv, 0.0f);
         } else {
             float tmp[9];
 #pragma unroll
             for (int i = 0; i < 9; ++i) tmp[i] = w[i];
-            boundary_offsets<S>(bc, g, t, X, Y, tmp, omega, sc, inv);
+            if (SH == 1 || (SH == 2 && g.shift_u))
+                boundary_offsets_shifted<S>(bc, g.nb, g.shift_base(Y), t, X, Y, tmp, omega, sc, inv);
+            else
+                boundary_offsets<S>(bc, g, t, X, Y, tmp, omega, sc, inv);
 #pragma unroll
             for (int i = 0; i < 9; ++i) w[i] = tmp[i];
         }
@@ -229,7 +312,7 @@ __global__ void __launch_bounds__(BX) k_collide_inplace(Geo g, S *__restrict__ b
     for (int i = 0; i < 9; ++i) f[i] = Work<S>::load(plane(buf, g, i)[o], i, inv);
     collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) plane(buf, g, i)[o] = Work<S>::store(f[i], i, sc);
+    for (int i = 0; i < 9; ++i) plane(buf, g, i)[o] = Work<S>::store(stored_out<S>(g, Y, i, f[i], sc), i, sc);
     if (g.perimeter(X, Y)) {
         const int p = g.pidx(X, Y);
 #pragma unroll
@@ -280,7 +363,7 @@ __global__ void __launch_bounds__(BX) k_pull(Geo g, const S *__restrict__ src, S
     }
     collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = Work<S>::store(f[i], i, sc);
+    for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = Work<S>::store(stored_out<S>(g, Y, i, f[i], sc), i, sc);
     if (edge) {
         const int p = g.pidx(X, Y);
 #pragma unroll
@@ -290,7 +373,7 @@ __global__ void __launch_bounds__(BX) k_pull(Geo g, const S *__restrict__ src, S
 }
 
 // Pull step of one node, any storage type (the general path of every pull kernel).
-template <class S>
+template <class S, int SH = 2>
 __device__ __forceinline__ void pull_node(const Geo &g, const S *__restrict__ src, S *__restrict__ dst,
                                           const uint8_t *__restrict__ tag, const double *__restrict__ bc,
                                           double omega, S *__restrict__ side, float sc, float inv,
@@ -312,9 +395,9 @@ __device__ __forceinline__ void pull_node(const Geo &g, const S *__restrict__ sr
                                                     : side[(size_t)i * g.nper + p], i, inv);
         }
     }
-    collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
+    collide_w<S, SH>(bc, g, tag[o], X, Y, f, omega, sc, inv);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = Work<S>::store(f[i], i, sc);
+    for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = Work<S>::store(stored_out<S, SH>(g, Y, i, f[i], sc), i, sc);
     if (edge) {
 #pragma unroll
         for (int i = 0; i < 9; ++i)
@@ -332,7 +415,7 @@ __device__ __forceinline__ void pull_node(const Geo &g, const S *__restrict__ sr
 //
 // pull_quad runs the four nodes x0..x0+3 of row Y for one lane of a warp whose lanes cover 128
 // consecutive nodes (the choice between the vector and the per-node path is made per warp).
-template <class S>
+template <class S, bool SHIFT>
 __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ src, S *__restrict__ dst,
                                           const uint8_t *__restrict__ tag, const double *__restrict__ bc,
                                           double omega, S *__restrict__ side, float sc, float inv, int x0,
@@ -343,7 +426,7 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
     const bool vec = (xw0 >= 2) && (xw0 + 127 <= g.lx - 1) && (Y >= 2) && (Y <= g.ly - 1);
     if (!vec) {
         for (int k = 0; k < 4; ++k)
-            if (x0 + k <= g.lx) pull_node<S>(g, src, dst, tag, bc, omega, side, sc, inv, x0 + k, Y);
+            if (x0 + k <= g.lx) pull_node<S, SHIFT ? 1 : 0>(g, src, dst, tag, bc, omega, side, sc, inv, x0 + k, Y);
         return;
     }
     const long long o = g.idx(x0, Y);
@@ -375,15 +458,20 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
     }
     if (tq == 0x01010101u) {         // four bulk nodes
         const float om = (float)omega;
+        const float us = SHIFT ? g.shift_u[Y] : 0.0f;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) bgk_offsets(D[k], om, sc, inv);
+        for (int k = 0; k < 4; ++k) bgk_offsets<SHIFT>(D[k], om, sc, inv, us);
     } else {
 #pragma unroll
         for (int k = 0; k < 4; ++k)
-            collide_w<S>(bc, g, (int)((tq >> (8 * k)) & 0xff), x0 + k, Y, D[k], omega, sc, inv);
+            collide_w<S, SHIFT ? 1 : 0>(bc, g, (int)((tq >> (8 * k)) & 0xff), x0 + k, Y, D[k], omega, sc, inv);
     }
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
+        if (SHIFT) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) D[k][i] = stored_out<S, 1>(g, Y, i, D[k][i], sc);
+        }
         uint2 w;
         w.x = H::pack(D[0][i], D[1][i]);
         w.y = H::pack(D[2][i], D[3][i]);
@@ -392,15 +480,16 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
 }
 
 // Eight blocks of 128 threads a SM (64 registers): more loads in flight than the 72-register
-// allocation's seven, for a few bytes of spills on the per-node fallback path.
-template <class S>
-__global__ void __launch_bounds__(BX, 8) k_pull4h(Geo g, const S *__restrict__ src, S *__restrict__ dst,
+// allocation's seven, for a few bytes of spills on the per-node fallback path.  The shifted form
+// holds the row's rebase values as well and keeps seven (72 registers).
+template <class S, bool SHIFT>
+__global__ void __launch_bounds__(BX, SHIFT ? 7 : 8) k_pull4h(Geo g, const S *__restrict__ src, S *__restrict__ dst,
                                                const uint8_t *__restrict__ tag,
                                                const double *__restrict__ bc, double omega,
                                                S *__restrict__ side, float sc, float inv)
 {
     const int t = blockIdx.x * BX + threadIdx.x;
-    pull_quad<S>(g, src, dst, tag, bc, omega, side, sc, inv, 1 + 4 * t, blockIdx.y + 1, threadIdx.x & 31);
+    pull_quad<S, SHIFT>(g, src, dst, tag, bc, omega, side, sc, inv, 1 + 4 * t, blockIdx.y + 1, threadIdx.x & 31);
 }
 
 // Propagation of C_n in `src` into `dst` (form C -> form L), ghost ring included; stale
@@ -490,7 +579,7 @@ __global__ void __launch_bounds__(PULL2_THREADS) k_pull2(Geo g, const S *__restr
         }
         collide_w<S>(bc, g, tag[g.idx(X, Y)], X, Y, f, omega, sc, inv);
 #pragma unroll
-        for (int i = 0; i < 9; ++i) s1[i * T::N1 + k] = Work<S>::store(f[i], i, sc);
+        for (int i = 0; i < 9; ++i) s1[i * T::N1 + k] = Work<S>::store(stored_out<S>(g, Y, i, f[i], sc), i, sc);
         if (edge && X >= x0 && X < x0 + TW && Y >= y0 && Y < y0 + TH) {
 #pragma unroll
             for (int i = 0; i < 9; ++i)
@@ -516,7 +605,7 @@ __global__ void __launch_bounds__(PULL2_THREADS) k_pull2(Geo g, const S *__restr
         const long long o = g.idx(X, Y);
         collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
 #pragma unroll
-        for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = Work<S>::store(f[i], i, sc);
+        for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = Work<S>::store(stored_out<S>(g, Y, i, f[i], sc), i, sc);
         if (edge) {
 #pragma unroll
             for (int i = 0; i < 9; ++i)
@@ -573,7 +662,7 @@ __device__ __forceinline__ void aa_even_node(const Geo &g, S *__restrict__ a, co
     }
     collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) plane(a, g, opp(i))[o] = Work<S>::store(f[i], i, sc);
+    for (int i = 0; i < 9; ++i) plane(a, g, opp(i))[o] = Work<S>::store(stored_out<S>(g, Y, i, f[i], sc), i, sc);
     if (edge) {
 #pragma unroll
         for (int i = 0; i < 9; ++i)
@@ -610,7 +699,7 @@ __device__ __forceinline__ void aa_odd_node(const Geo &g, S *__restrict__ a, con
     collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
 #pragma unroll
     for (int i = 0; i < 9; ++i)
-        plane(a, g, i)[o + cx(i) + (long long)cy(i) * g.pitch] = Work<S>::store(f[i], i, sc);
+        plane(a, g, i)[o + cx(i) + (long long)cy(i) * g.pitch] = Work<S>::store(stored_out<S>(g, Y, i, f[i], sc), i, sc);
     if (edge) {
 #pragma unroll
         for (int i = 0; i < 9; ++i)
@@ -684,8 +773,12 @@ __device__ __forceinline__ void batch_node(const BatchInst *__restrict__ insts, 
             const int lane = threadIdx.x & 31;
             S *side = static_cast<S *>(d.side) + (size_t)((d.tau0 + k) & 1) * 9 * (size_t)g.nper;
             const int src = d.cur0 ^ (k & 1);
-            pull_quad<S>(g, static_cast<const S *>(d.buf[src]), static_cast<S *>(d.buf[src ^ 1]), d.tag,
-                         d.bc, d.omega, side, d.scale, d.inv_scale, it.x0 + 4 * lane, Y, lane);
+            if (g.shift_u)
+                pull_quad<S, true>(g, static_cast<const S *>(d.buf[src]), static_cast<S *>(d.buf[src ^ 1]),
+                                   d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, it.x0 + 4 * lane, Y, lane);
+            else
+                pull_quad<S, false>(g, static_cast<const S *>(d.buf[src]), static_cast<S *>(d.buf[src ^ 1]),
+                                    d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, it.x0 + 4 * lane, Y, lane);
         }
         return;
     }
@@ -786,7 +879,7 @@ __global__ void __launch_bounds__(BX) k_upload(Geo g, const double *__restrict__
     const long long o = g.idx(X, Y);
 #pragma unroll
     for (int i = 0; i < 9; ++i)
-        plane(buf, g, i)[o] = Codec<S>::enc((typename Codec<S>::R)in[r + i], i, sc);
+        plane(buf, g, i)[o] = enc_row<S>(g, (typename Codec<S>::R)in[r + i], i, sc, Y);
 }
 
 // ---- outlet extrapolation, periodic wrap, initial state, macroscopic fields ---------------
@@ -868,7 +961,7 @@ __global__ void __launch_bounds__(BX) k_init_cylinder(Geo g, S *__restrict__ buf
         rules::equilibrium<double>(f, 1.0, u, 0.0);
 #pragma unroll
         for (int i = 0; i < 9; ++i)
-            plane(buf, g, i)[o] = Codec<S>::enc((typename Codec<S>::R)f[i], i, sc);
+            plane(buf, g, i)[o] = enc_row<S>(g, (typename Codec<S>::R)f[i], i, sc, Y);
     } else {
 #pragma unroll
         for (int i = 0; i < 9; ++i) plane(buf, g, i)[o] = S(0);
@@ -1095,6 +1188,17 @@ void launch_collide_inplace(const DevLattice &d, int cur, int side_par, cudaStre
                        d.omega, SIDE<S>(d, side_par), d.scale, d.inv_scale)));
 }
 
+template <class S>
+static void launch_pull4h(const DevLattice &d, dim3 grid, int src, int side_par, cudaStream_t s)
+{
+    if (d.g.shift_u)
+        k_pull4h<S, true><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
+                                              SIDE<S>(d, side_par), d.scale, d.inv_scale);
+    else
+        k_pull4h<S, false><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
+                                               SIDE<S>(d, side_par), d.scale, d.inv_scale);
+}
+
 void launch_pull(const DevLattice &d, int src, int side_par, bool ghosts, cudaStream_t s)
 {
     if (ghosts) {
@@ -1103,15 +1207,8 @@ void launch_pull(const DevLattice &d, int src, int side_par, bool ghosts, cudaSt
                            d.tag, d.bc, d.omega, SIDE<S>(d, side_par), d.scale, d.inv_scale)));
     } else if (d.precision == LBGPU_F16 || d.precision == LBGPU_BF16) {
         dim3 grid(cdiv((d.g.lx + 3) / 4, BX), d.g.ly);
-        if (d.precision == LBGPU_F16)
-            k_pull4h<__half><<<grid, BX, 0, s>>>(d.g, B<__half>(d, src), B<__half>(d, 1 - src), d.tag,
-                                                 d.bc, d.omega, SIDE<__half>(d, side_par), d.scale,
-                                                 d.inv_scale);
-        else
-            k_pull4h<__nv_bfloat16><<<grid, BX, 0, s>>>(d.g, B<__nv_bfloat16>(d, src),
-                                                        B<__nv_bfloat16>(d, 1 - src), d.tag, d.bc,
-                                                        d.omega, SIDE<__nv_bfloat16>(d, side_par),
-                                                        d.scale, d.inv_scale);
+        if (d.precision == LBGPU_F16) launch_pull4h<__half>(d, grid, src, side_par, s);
+        else launch_pull4h<__nv_bfloat16>(d, grid, src, side_par, s);
     } else {
         dim3 grid(cdiv(d.g.lx, BX), d.g.ly);
         LBGPU_DISPATCH(d, (k_pull<S, false><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src),

@@ -130,7 +130,8 @@ void Lattice::destroy()
     if (stage) cudaFree(stage);
     if (red_scratch) cudaFree(red_scratch);
     if (vel_acc) cudaFree(vel_acc);
-    red_scratch = nullptr; vel_acc = nullptr; vel_samples = 0;
+    if (shift) cudaFree(shift);
+    red_scratch = nullptr; vel_acc = nullptr; vel_samples = 0; shift = nullptr;
     if (stream) cudaStreamDestroy(stream);
     d = DevLattice{};
     stage = nullptr; stage_bytes = 0; stream = nullptr;

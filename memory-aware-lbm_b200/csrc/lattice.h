@@ -68,6 +68,7 @@ struct Lattice {
     int velocity_average(double *ux, double *uy, long long *samples);
     double *red_scratch = nullptr;  // (ly+2)*8 partial sums + 8 results
     double *vel_acc = nullptr;      // 2*lx*ly running velocity sums
+    float *shift = nullptr;         // 16-bit storage: per-row shift velocity [ly+2] (d.g.shift_u)
     long long vel_samples = 0;
     int check(const char *what);   // cudaGetLastError -> error code
     int side_par_stale() const { return (int)((n + 1) & 1); }

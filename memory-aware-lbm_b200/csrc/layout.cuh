@@ -25,6 +25,16 @@ struct Geo {
     int nper;        // perimeter side-store stride, 2*lx + 2*ly
     long long pitch; // elements per row
     long long plane; // elements per direction plane, (ly + 2) * pitch
+    // 16-bit storage only: the per-row shift table (device), or null.  Stored values are then
+    // relative to S_i(Y) = f_eq_i(1, (u_s(Y), 0)) of the row that consumes them instead of to
+    // w_i.  Layout, all float, Y = 0..ly+1: u_s[Y]; base[Y][9] = S_i(Y); rebase[Y][9] =
+    // S_i(Y) - S_i(Y + c_iy) (0 where c_iy = 0 or the row is a ghost row).
+    const float *shift_u;
+    __host__ __device__ __forceinline__ const float *shift_base(int Y) const { return shift_u + (ly + 2) + 9 * Y; }
+    __host__ __device__ __forceinline__ const float *shift_rebase(int Y) const
+    {
+        return shift_u + 10 * (ly + 2) + 9 * Y;
+    }
 
     __host__ __device__ __forceinline__ long long idx(int X, int Y) const
     {
@@ -69,6 +79,7 @@ inline Geo make_geo(int lx, int ly, int elem_bytes)
     g.plane = (long long)(ly + 2) * g.pitch;
     g.nb = (lx > ly ? lx : ly) + 2;
     g.nper = 2 * lx + 2 * ly;
+    g.shift_u = nullptr;
     return g;
 }
 

@@ -1,6 +1,7 @@
 // native.cu -- the lbgpu_* functions of include/lbgpu.h (lattice object interface).
 #include <cstring>
 #include <vector>
+#include "d2q9.cuh"
 #include "lattice.h"
 #include "lbgpu.h"
 
@@ -120,6 +121,53 @@ int lbgpu_set_offset_scale(lbgpu_lattice *h, int scale_log2)
         return set_error(LB_ERR_ARG, "offset scale 2^%d out of range", scale_log2);
     h->L.d.scale = ldexpf(1.0f, scale_log2);
     h->L.d.inv_scale = ldexpf(1.0f, -scale_log2);
+    return LB_OK;
+}
+
+int lbgpu_set_offset_shift(lbgpu_lattice *h, const double *u_row)
+{
+    if (int rc = bad_handle(h, "lbgpu_set_offset_shift")) return rc;
+    Lattice &L = h->L;
+    if (L.precision != LBGPU_F16 && L.precision != LBGPU_BF16)
+        return set_error(LB_ERR_STATE, "lbgpu_set_offset_shift: FP16/BF16 storage only");
+    if (!u_row) {
+        if (L.shift) {
+            if (int rc = lbgpu::cuda_error(cudaStreamSynchronize(L.stream), "lbgpu_set_offset_shift")) return rc;
+            cudaFree(L.shift);
+        }
+        L.shift = nullptr;
+        L.d.g.shift_u = nullptr;
+        return LB_OK;
+    }
+    // the table of Geo::shift_u: u_s[Y], S_i(Y), S_i(Y) - S_i(Y + c_iy) (layout.cuh), in FP64
+    // from the float velocities, then rounded once, so every kernel reads the same values
+    const int ny2 = L.ly + 2;
+    std::vector<float> u(19 * (size_t)ny2, 0.0f);
+    for (int Y = 0; Y < ny2; ++Y) {
+        if (!(u_row[Y] > -0.5 && u_row[Y] < 0.5))
+            return set_error(LB_ERR_ARG, "lbgpu_set_offset_shift: u[%d] = %g out of range", Y, u_row[Y]);
+        u[Y] = (float)u_row[Y];
+    }
+    auto S = [&](int i, int Y) {
+        const double v = (double)u[Y], c = (double)lbgpu::cx(i), w = (double)lbgpu::wgtf(i);
+        return w * (1.0 + 3.0 * c * v + 4.5 * c * c * v * v - 1.5 * v * v);
+    };
+    for (int Y = 0; Y < ny2; ++Y)
+        for (int i = 0; i < 9; ++i) {
+            u[ny2 + 9 * Y + i] = (float)S(i, Y);
+            const int Yc = Y + lbgpu::cy(i);
+            if (lbgpu::cy(i) != 0 && Yc >= 0 && Yc < ny2) u[10 * ny2 + 9 * Y + i] = (float)(S(i, Y) - S(i, Yc));
+        }
+    if (!L.shift) {
+        void *p = nullptr;
+        if (int rc = lbgpu::cuda_error(cudaMalloc(&p, u.size() * sizeof(float)), "cudaMalloc(offset shift)")) return rc;
+        L.shift = static_cast<float *>(p);
+    }
+    if (int rc = lbgpu::cuda_error(cudaMemcpyAsync(L.shift, u.data(), u.size() * sizeof(float),
+                                                   cudaMemcpyHostToDevice, L.stream), "upload offset shift"))
+        return rc;
+    if (int rc = lbgpu::cuda_error(cudaStreamSynchronize(L.stream), "upload offset shift")) return rc;
+    L.d.g.shift_u = L.shift;
     return LB_OK;
 }
 

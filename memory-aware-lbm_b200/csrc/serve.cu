@@ -61,6 +61,7 @@ struct lbgpu_server {
     size_t budget = 0;
     int check_every = 100;
     int scale_log2 = 10;
+    bool shift = false;                      // 16-bit offsets from each request's inflow profile
     std::vector<Req> reqs;
     unsigned *d_change = nullptr;
     int cap_change = 0;
@@ -91,8 +92,18 @@ int start(lbgpu_server *s, Req &q)
     const lbgpu_request &r = q.spec;
     const int sch = scheme_of(s, r);
     if (int rc = lbgpu_create(r.lx, r.ly, s->precision, sch, &q.lat)) return rc;
-    if (s->precision == LBGPU_F16 || s->precision == LBGPU_BF16)
+    if (s->precision == LBGPU_F16 || s->precision == LBGPU_BF16) {
         if (int rc = lbgpu_set_offset_scale(q.lat, s->scale_log2)) return rc;
+        if (s->shift) {   // the channel's Poiseuille inflow profile, as lbgpu_setup_cylinder writes it
+            std::vector<double> u(r.ly + 2, 0.0);
+            const double L = r.ly - 1.0;
+            for (int Y = 1; Y <= r.ly; ++Y) {
+                const double y = Y - 1.0;
+                u[Y] = 4.0 * r.umax / (L * L) * (L * y - y * y);
+            }
+            if (int rc = lbgpu_set_offset_shift(q.lat, u.data())) return rc;
+        }
+    }
     if (int rc = lbgpu_setup_cylinder(q.lat, r.obst_x, r.obst_y, r.obst_r, r.umax, r.re,
                                       LBGPU_WALL_BOUNCEBACK, LBGPU_OUTLET_CONST, nullptr))
         return rc;
@@ -210,6 +221,15 @@ int lbgpu_server_set_solo_nodes(lbgpu_server *s, long long nodes)
 {
     if (!s || nodes < 0) return set_error(LB_ERR_ARG, "lbgpu_server_set_solo_nodes: bad arguments");
     s->solo_nodes = nodes;
+    return LB_OK;
+}
+
+int lbgpu_server_set_offset_shift(lbgpu_server *s, int on)
+{
+    if (!s) return set_error(LB_ERR_ARG, "lbgpu_server_set_offset_shift: null server");
+    if (on && s->precision != LBGPU_F16 && s->precision != LBGPU_BF16)
+        return set_error(LB_ERR_STATE, "lbgpu_server_set_offset_shift: FP16/BF16 storage only");
+    s->shift = on != 0;
     return LB_OK;
 }
 

@@ -82,6 +82,7 @@ def lib():
     L.lbgpu_set_geometry.argtypes = [_vp, ctypes.c_double, _u8p, _dp, _u8p]
     L.lbgpu_set_populations.argtypes = [_vp, _dp, _dp]
     L.lbgpu_set_offset_scale.argtypes = [_vp, ctypes.c_int]
+    L.lbgpu_set_offset_shift.argtypes = [_vp, _dp]
     L.lbgpu_setup_cylinder.argtypes = [_vp] + [ctypes.c_int] * 3 + [ctypes.c_double] * 2 + [
         ctypes.c_int] * 2 + [_dp]
     L.lbgpu_build_cylinder.restype = ctypes.c_double
@@ -129,6 +130,7 @@ def lib():
     L.lbgpu_server_set_persistent.argtypes = [_vp, ctypes.c_int]
     L.lbgpu_server_set_threads.argtypes = [_vp, ctypes.c_int]
     L.lbgpu_server_set_solo_nodes.argtypes = [_vp, ctypes.c_longlong]
+    L.lbgpu_server_set_offset_shift.argtypes = [_vp, ctypes.c_int]
     L.lbgpu_server_set_offset_scale.argtypes = [_vp, ctypes.c_int]
     L.lbgpu_server_submit.argtypes = [_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int)]
     L.lbgpu_server_run.argtypes = [_vp, ctypes.c_int]
@@ -227,6 +229,16 @@ class Lattice:
     def set_offset_scale(self, scale_log2):
         _check(lib().lbgpu_set_offset_scale(self.h, int(scale_log2)))
 
+    def set_offset_shift(self, u_row):
+        """Per-row shift velocity of FP16/BF16 offsets (ly + 2 values), or None for w_i."""
+        if u_row is None:
+            _check(lib().lbgpu_set_offset_shift(self.h, None))
+            return
+        u = np.ascontiguousarray(u_row, np.float64)
+        if u.shape != (self.ly + 2,):
+            raise ValueError(f"shift profile needs {self.ly + 2} values")
+        _check(lib().lbgpu_set_offset_shift(self.h, _p(u)))
+
     def setup_cylinder(self, obst_x, obst_y, obst_r, umax=0.02, re=100.0, wall=WALL_REGULARIZED,
                        outlet=OUTLET_ZGB):
         om = ctypes.c_double()
@@ -306,6 +318,20 @@ class Lattice:
 
 
 DEFAULT_SCALE = {"f16": 10, "bf16": 6}
+# With a row shift the stored deviations are far smaller (down to ~1e-7 of f in a smooth far
+# field) while at most ~0.03: 2^17 keeps FP16 out of its subnormal range with a 15x margin below
+# its largest value.  BF16 has FP32's exponent range, so its scale does not matter.
+DEFAULT_SHIFT_SCALE = {"f16": 17, "bf16": 6}
+
+
+def poiseuille_profile(ly, umax):
+    """The cylinder channel's inflow profile per row Y = 0..ly+1 (0 in the ghost rows): the
+    natural per-row shift of 16-bit offsets for that channel (lbgpu_set_offset_shift)."""
+    u = np.zeros(ly + 2)
+    L = ly - 1.0
+    y = np.arange(ly, dtype=np.float64)
+    u[1:ly + 1] = 4.0 * umax / (L * L) * (L * y - y * y)
+    return u
 
 
 def cylinder_lattice(lx, ly, precision="f64", scheme="pull", umax=0.02, re=100.0,
@@ -458,7 +484,8 @@ def lattice_bytes(lx, ly, precision="f32", scheme="pull"):
 class Server:
     """lbgpu_server: continuous batching of cylinder-channel requests under an HBM budget."""
 
-    def __init__(self, precision="f32", budget_bytes=8 << 30, check_every=100, scale=None):
+    def __init__(self, precision="f32", budget_bytes=8 << 30, check_every=100, scale=None,
+                 shift=False):
         self.precision = precision
         h = _vp()
         _check(lib().lbgpu_server_create(PRECISIONS[precision], int(budget_bytes),
@@ -466,8 +493,10 @@ class Server:
         self.h = h
         self.requests = []
         if precision in DEFAULT_SCALE:
-            _check(lib().lbgpu_server_set_offset_scale(
-                h, DEFAULT_SCALE[precision] if scale is None else int(scale)))
+            default = (DEFAULT_SHIFT_SCALE if shift else DEFAULT_SCALE)[precision]
+            _check(lib().lbgpu_server_set_offset_scale(h, default if scale is None else int(scale)))
+            if shift:
+                _check(lib().lbgpu_server_set_offset_shift(h, 1))
 
     def close(self):
         if self.h:

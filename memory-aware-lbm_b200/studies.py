@@ -10,8 +10,9 @@ batching   independent channels of uneven size, Reynolds number and obstacle pla
 serving    a Poisson stream of channel requests through lbgpu_server: continuous batching under
            an HBM budget against sequential plain solves of the same requests; p50/p99 latency,
            aggregate MLUPS, and the velocity error of a sample against FP64 re-runs.
-precision  one large channel stored as FP16 or BF16 offsets against the FP64 kernel: relative
-           L2 error of the time-averaged velocity, mass drift, drag and lift coefficients.
+precision  one large channel stored as FP16 or BF16 offsets (from w_i, or with the suffix "s"
+           from the inflow profile's equilibrium per row) against the FP64 kernel: relative L2
+           error of the time-averaged velocity, mass drift, drag and lift coefficients.
 """
 from __future__ import annotations
 
@@ -49,10 +50,13 @@ def batching_instances(n=512, seed=20260101):
     return out
 
 
-def _channel(q, precision, scheme):
+def _channel(q, precision, scheme, shift=None):
     lat = lbgpu.Lattice(q["lx"], q["ly"], precision, scheme)
     if precision in lbgpu.DEFAULT_SCALE:
-        lat.set_offset_scale(lbgpu.DEFAULT_SCALE[precision])
+        scales = lbgpu.DEFAULT_SCALE if shift is None else lbgpu.DEFAULT_SHIFT_SCALE
+        lat.set_offset_scale(scales[precision])
+    if shift is not None:
+        lat.set_offset_shift(shift)
     lat.setup_cylinder(q["obst_x"], q["obst_y"], q["obst_r"], q["umax"], q["re"],
                        lbgpu.WALL_BOUNCEBACK, lbgpu.OUTLET_CONST)
     return lat
@@ -150,8 +154,8 @@ def serving_requests(n, seed=20260102, nmin=1e4, nmax=2e7, max_steps=5000, tol=1
     return out
 
 
-def _serve(prec, reqs, batched, budget, schemes=None, shapes=None, sample=()):
-    with lbgpu.Server(prec, budget, 100) as srv:
+def _serve(prec, reqs, batched, budget, schemes=None, shapes=None, sample=(), shift=False):
+    with lbgpu.Server(prec, budget, 100, shift=shift and prec in lbgpu.DEFAULT_SCALE) as srv:
         for c, s in (schemes or {}).items():
             srv.set_scheme(c, s)
         for c, (w, npt) in (shapes or {}).items():
@@ -172,12 +176,13 @@ def _serve(prec, reqs, batched, budget, schemes=None, shapes=None, sample=()):
 
 
 def serving_study(precisions=("f32", "f16"), n=120, seed=20260102, budget_gb=150.0,
-                  load=0.95, sample_every=50):
+                  load=0.95, sample_every=50, shift=0):
+    """shift=1: FP16/BF16 requests store offsets from their inflow profile (row shift)."""
     reqs = serving_requests(n, seed)
     work = [q["lx"] * q["ly"] * q["max_steps"] for q in reqs]
     budget = int(budget_gb * 1e9)
     sample = set(range(0, n, sample_every))
-    out = {"requests": n, "seed": seed, "budget_gb": budget_gb, "offered_load": load,
+    out = {"requests": n, "seed": seed, "budget_gb": budget_gb, "offered_load": load, "row_shift": bool(shift),
            "nodes_log_uniform": [1e4, 2e7], "max_steps": 5000, "tol": 1e-7,
            "fp64_sample": sorted(sample), "precisions": {}}
     rng = np.random.default_rng(seed + 1)
@@ -186,16 +191,16 @@ def serving_study(precisions=("f32", "f16"), n=120, seed=20260102, budget_gb=150
         schemes = {c: v["scheme"] for c, v in
                    tune_schemes(prec, [(q["lx"], q["ly"]) for q in reqs]).items()}
         # capacity: the batched rate on the whole request set at once (all arrive at t=0)
-        closed, _ = _serve(prec, reqs, True, budget, schemes)
+        closed, _ = _serve(prec, reqs, True, budget, schemes, shift=shift)
         cap = closed["mlups"] * 1e6
         mean_work = float(np.mean(work))
         rate = load * cap / mean_work            # requests per second
         t = np.cumsum(rng.exponential(1.0 / rate, n))
         stream = [dict(q, arrival=float(t[k] - t[0])) for k, q in enumerate(reqs)]
-        served, res = _serve(prec, stream, True, budget, schemes, sample=sample)
+        served, res = _serve(prec, stream, True, budget, schemes, sample=sample, shift=shift)
         # sequential plain solves: each request alone with the single-lattice pull kernel
-        seq, _ = _serve(prec, stream, False, budget)
-        seq_closed, _ = _serve(prec, reqs, False, budget)
+        seq, _ = _serve(prec, stream, False, budget, shift=shift)
+        seq_closed, _ = _serve(prec, reqs, False, budget, shift=shift)
         errs = []
         for k in sorted(sample):
             q = reqs[k]
@@ -224,10 +229,16 @@ def serving_study(precisions=("f32", "f16"), n=120, seed=20260102, budget_gb=150
 # ------------------------------------------------------------------------------------------
 # precision
 # ------------------------------------------------------------------------------------------
+def _storage(name):
+    """'f16s' / 'bf16s': 16-bit offsets from the channel's Poiseuille profile (row shift)."""
+    return (name[:-1], True) if name.endswith("s") else (name, False)
+
+
 def _run_averaged(nx, ny, prec, umax, re, steps, avg_every, moment_every):
     ox, oy, r = nx // 5 + 1, ny // 2 + 1, ny // 10 + 1
     q = dict(lx=nx, ly=ny, obst_x=ox, obst_y=oy, obst_r=r, umax=umax, re=re)
-    with _channel(q, prec, "pull") as lat:
+    base, shifted = _storage(prec)
+    with _channel(q, base, "pull", lbgpu.poiseuille_profile(ny, umax) if shifted else None) as lat:
         m0 = lat.moments()
         half = steps // 2
         ms = lat.step_timed(half)
@@ -253,7 +264,7 @@ def _run_averaged(nx, ny, prec, umax, re, steps, avg_every, moment_every):
 
 
 def precision_study(nx=16384, ny=4096, steps=20000, cases=((100.0, 0.02), (1000.0, 0.05)),
-                    precisions=("f16", "bf16"), avg_every=10, moment_every=100):
+                    precisions=("f16", "bf16", "f16s", "bf16s"), avg_every=10, moment_every=100):
     out = {"nx": nx, "ny": ny, "steps": steps, "average": f"every {avg_every} steps over the "
            f"second half", "forces": f"momentum exchange every {moment_every} steps over the "
            "second half; C = F / (0.5 rho U^2 D), U = 2/3 uMax, D = 2r", "cases": []}
@@ -274,7 +285,10 @@ def precision_study(nx=16384, ny=4096, steps=20000, cases=((100.0, 0.02), (1000.
                           "cd_rel_err": abs(r["cd"] - ref["cd"]) / abs(ref["cd"]),
                           "cl_abs_err": abs(r["cl"] - ref["cl"]),
                           "non_finite": r["non_finite"],
-                          "scale_log2": lbgpu.DEFAULT_SCALE[prec]}
+                          "scale_log2": (lbgpu.DEFAULT_SHIFT_SCALE if _storage(prec)[1]
+                                         else lbgpu.DEFAULT_SCALE)[_storage(prec)[0]],
+                          "offsets_from": "Poiseuille-profile equilibrium per row" if _storage(prec)[1]
+                          else "w_i"}
             del r
         out["cases"].append(case)
         del ref
