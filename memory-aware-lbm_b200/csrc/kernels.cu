@@ -514,13 +514,9 @@ __global__ void __launch_bounds__(BX) k_stream(Geo g, const S *__restrict__ src,
 
 // ---- two steps per sweep (temporal blocking) ----------------------------------------------
 //
-// The GPU form of the reference's two-steps-per-sweep ("tight") idea (lb.c:442-572): a block
-// loads the collided state C_n of its TW x TH tile and a two-node halo into shared memory,
-// computes C_{n+1} on the tile and a one-node halo (the halo redundantly with the neighbouring
-// blocks: the same per-node function, so the same values), then C_{n+2} on the tile, and writes
-// only that to the other buffer.  DRAM sees one read and one write of the lattice per two
-// steps.  Each node runs pull_node's arithmetic on the same inputs, and the intermediate state
-// is kept in the storage type, so the result is identical to two single pull steps.
+// The GPU form of the reference's two-steps-per-sweep ("tight") idea (lb.c:442-572).  Each node
+// runs pull_node's arithmetic on the same inputs and the intermediate state is kept in the
+// storage type, so the result is identical to two single pull steps.
 //
 // Stale slots: step n+1 reads side parity (n+1)&1 (C_{n-1}); its new values go to the scratch
 // slot `side_tmp`, not to that parity, because neighbouring blocks may still read it for their
@@ -528,93 +524,101 @@ __global__ void __launch_bounds__(BX) k_stream(Geo g, const S *__restrict__ src,
 // moves the scratch into parity (n+1)&1 and swaps the two buffers' ghost rings: the state ends
 // in the buffer two single steps would not have left it in, and the read-outs take ghost values
 // from the other buffer.
-template <int TW, int TH> struct Tile2 {
-    static constexpr int W0 = TW + 4, H0 = TH + 4;    // C_n region, origin (x0 - 2, y0 - 2)
-    static constexpr int W1 = TW + 2, H1 = TH + 2;    // C_{n+1} region, origin (x0 - 1, y0 - 1)
-    static constexpr int N0 = W0 * H0, N1 = W1 * H1;
-};
+//
+// The kernel is a sweep (the shape of the reference's tight variants): a block of W threads owns a strip of W columns and a segment of H rows and walks down it,
+// keeping three rows of C_n (W + 4 wide) and three rows of C_{n+1} (W + 2 wide) in shared
+// memory.  Iteration t loads C_n row YL = y0 - 2 + t, computes C_{n+1} on row YL - 1 and C_{n+2}
+// on row YL - 2, which it writes.  Halo work is two columns a side and two rows a segment end
+// (a few percent), and the shared memory a block needs is small enough for several blocks a SM.
+template <class S, int W>
+constexpr size_t sweep2_r0_bytes() { return (3 * 9 * (size_t)(W + 4) * sizeof(S) + 15) / 16 * 16; }
+template <class S, int W>
+constexpr size_t sweep2_smem_bytes() { return sweep2_r0_bytes<S, W>() + 3 * 9 * (size_t)(W + 2) * sizeof(S); }
 
-template <class S, int TW, int TH>
-constexpr size_t pull2_smem_bytes() { return 9 * (size_t)(Tile2<TW, TH>::N0 + Tile2<TW, TH>::N1) * sizeof(S); }
-
-constexpr int PULL2_THREADS = 256;
-
-template <class S, int TW, int TH>
-__global__ void __launch_bounds__(PULL2_THREADS) k_pull2(Geo g, const S *__restrict__ src, S *__restrict__ dst,
-                                                        const uint8_t *__restrict__ tag,
-                                                        const double *__restrict__ bc, double omega,
-                                                        const S *__restrict__ side_a, S *__restrict__ side_tmp,
-                                                        S *__restrict__ side_b, float sc, float inv)
+template <class S, int W, int H>
+__global__ void __launch_bounds__(W) k_sweep2(Geo g, const S *__restrict__ src, S *__restrict__ dst,
+                                             const uint8_t *__restrict__ tag, const double *__restrict__ bc,
+                                             double omega, const S *__restrict__ side_a,
+                                             S *__restrict__ side_tmp, S *__restrict__ side_b, float sc,
+                                             float inv)
 {
-    using T = Tile2<TW, TH>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    S *s0 = reinterpret_cast<S *>(smem_raw);          // [9][H0][W0]
-    S *s1 = s0 + 9 * T::N0;                           // [9][H1][W1]
-    const int x0 = 1 + blockIdx.x * TW, y0 = 1 + blockIdx.y * TH;
-    const int tid = threadIdx.x;
-
-    // C_n of the tile and its two-node halo (positions outside the array are never read)
-#pragma unroll 4
-    for (int k = tid; k < 9 * T::N0; k += PULL2_THREADS) {
-        const int i = k / T::N0, rc = k - i * T::N0;
-        const int r = rc / T::W0, c = rc - r * T::W0;
-        const int X = x0 - 2 + c, Y = y0 - 2 + r;
-        if (X >= 0 && X <= g.lx + 1 && Y >= 0 && Y <= g.ly + 1) s0[k] = plane(src, g, i)[g.idx(X, Y)];
-    }
-    __syncthreads();
-
-    // step n+1 on the tile and a one-node halo, into shared memory
-    for (int k = tid; k < T::N1; k += PULL2_THREADS) {
-        const int r = k / T::W1, c = k - r * T::W1;
-        const int X = x0 - 1 + c, Y = y0 - 1 + r;
-        if (!g.interior(X, Y)) continue;
-        const bool edge = g.perimeter(X, Y);
-        const int p = edge ? g.pidx(X, Y) : 0;
-        typename Work<S>::W f[9];
+    constexpr int W0 = W + 4, W1 = W + 2;
+    extern __shared__ __align__(16) unsigned char sweep_smem[];
+    auto r0 = reinterpret_cast<S (*)[9][W0]>(sweep_smem);                 // C_n rows [3], slot = row mod 3
+    auto r1 = reinterpret_cast<S (*)[9][W1]>(sweep_smem + sweep2_r0_bytes<S, W>());   // C_{n+1} rows [3]
+    const int x0 = 1 + blockIdx.x * W, y0 = 1 + blockIdx.y * H;
+    const int tx = threadIdx.x;
+    const int yend = min(y0 + H, g.ly + 1);           // rows y0 .. yend-1 are this block's
+    for (int t = 0; y0 - 2 + t - 2 < yend; ++t) {
+        const int YL = y0 - 2 + t;
+        // C_n row YL (positions outside the array are never read)
+        if (YL >= 0 && YL <= g.ly + 1) {
+            const int sl = (YL + 3) % 3;
+            for (int k = tx; k < W0; k += W) {
+                const int X = x0 - 2 + k;
+                if (X >= 0 && X <= g.lx + 1) {
+                    const long long o = g.idx(X, YL);
 #pragma unroll
-        for (int i = 0; i < 9; ++i) {
-            const int sx = X - cx(i), sy = Y - cy(i);
-            f[i] = Work<S>::load(g.interior(sx, sy) ? s0[i * T::N0 + (sy - y0 + 2) * T::W0 + (sx - x0 + 2)]
-                                                    : side_a[(size_t)i * g.nper + p], i, inv);
+                    for (int i = 0; i < 9; ++i) r0[sl][i][k] = plane(src, g, i)[o];
+                }
+            }
         }
-        collide_w<S>(bc, g, tag[g.idx(X, Y)], X, Y, f, omega, sc, inv);
+        __syncthreads();
+        // step n+1 on row YL - 1, columns x0-1 .. x0+W
+        const int Y1 = YL - 1;
+        if (Y1 >= y0 - 1 && Y1 >= 1 && Y1 <= g.ly && Y1 <= yend) {
+            for (int k = tx; k < W1; k += W) {
+                const int X = x0 - 1 + k;
+                if (X < 1 || X > g.lx) continue;
+                const bool edge = g.perimeter(X, Y1);
+                const int p = edge ? g.pidx(X, Y1) : 0;
+                typename Work<S>::W f[9];
 #pragma unroll
-        for (int i = 0; i < 9; ++i) s1[i * T::N1 + k] = Work<S>::store(stored_out<S>(g, Y, i, f[i], sc), i, sc);
-        if (edge && X >= x0 && X < x0 + TW && Y >= y0 && Y < y0 + TH) {
+                for (int i = 0; i < 9; ++i) {
+                    const int sx = X - cx(i), sy = Y1 - cy(i);
+                    f[i] = Work<S>::load(g.interior(sx, sy) ? r0[(sy + 3) % 3][i][sx - x0 + 2]
+                                                            : side_a[(size_t)i * g.nper + p], i, inv);
+                }
+                collide_w<S>(bc, g, tag[g.idx(X, Y1)], X, Y1, f, omega, sc, inv);
+                const int sl = (Y1 + 3) % 3;
 #pragma unroll
-            for (int i = 0; i < 9; ++i)
-                if (!g.interior(X - cx(i), Y - cy(i))) side_tmp[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
+                for (int i = 0; i < 9; ++i) r1[sl][i][k] = Work<S>::store(stored_out<S>(g, Y1, i, f[i], sc), i, sc);
+                if (edge && X >= x0 && X < x0 + W && Y1 >= y0 && Y1 < yend) {
+#pragma unroll
+                    for (int i = 0; i < 9; ++i)
+                        if (!g.interior(X - cx(i), Y1 - cy(i)))
+                            side_tmp[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
+                }
+            }
         }
-    }
-    __syncthreads();
-
-    // step n+2 on the tile, to the other buffer
-    for (int k = tid; k < TW * TH; k += PULL2_THREADS) {
-        const int r = k / TW, c = k - r * TW;
-        const int X = x0 + c, Y = y0 + r;
-        if (X > g.lx || Y > g.ly) continue;
-        const bool edge = g.perimeter(X, Y);
-        const int p = edge ? g.pidx(X, Y) : 0;
-        typename Work<S>::W f[9];
+        __syncthreads();
+        // step n+2 on row YL - 2, columns x0 .. x0+W-1, to the other buffer
+        const int Y2 = YL - 2;
+        const int X = x0 + tx;
+        if (Y2 >= y0 && Y2 < yend && X <= g.lx) {
+            const bool edge = g.perimeter(X, Y2);
+            const int p = edge ? g.pidx(X, Y2) : 0;
+            typename Work<S>::W f[9];
 #pragma unroll
-        for (int i = 0; i < 9; ++i) {
-            const int sx = X - cx(i), sy = Y - cy(i);
-            f[i] = Work<S>::load(g.interior(sx, sy) ? s1[i * T::N1 + (sy - y0 + 1) * T::W1 + (sx - x0 + 1)]
-                                                    : side_b[(size_t)i * g.nper + p], i, inv);
-        }
-        const long long o = g.idx(X, Y);
-        collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
+            for (int i = 0; i < 9; ++i) {
+                const int sx = X - cx(i), sy = Y2 - cy(i);
+                f[i] = Work<S>::load(g.interior(sx, sy) ? r1[(sy + 3) % 3][i][sx - x0 + 1]
+                                                        : side_b[(size_t)i * g.nper + p], i, inv);
+            }
+            const long long o = g.idx(X, Y2);
+            collide_w<S>(bc, g, tag[o], X, Y2, f, omega, sc, inv);
 #pragma unroll
-        for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = Work<S>::store(stored_out<S>(g, Y, i, f[i], sc), i, sc);
-        if (edge) {
+            for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = Work<S>::store(stored_out<S>(g, Y2, i, f[i], sc), i, sc);
+            if (edge) {
 #pragma unroll
-            for (int i = 0; i < 9; ++i)
-                if (!g.interior(X - cx(i), Y - cy(i))) side_b[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
+                for (int i = 0; i < 9; ++i)
+                    if (!g.interior(X - cx(i), Y2 - cy(i))) side_b[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
+            }
         }
     }
 }
 
-// After k_pull2: the scratch stale slots into parity (n+1)&1, and the ghost rings of the two
+// After k_sweep2: the scratch stale slots into parity (n+1)&1, and the ghost rings of the two
 // buffers exchanged (one thread per perimeter node and per ghost-ring node).
 template <class S>
 __global__ void k_pull2_finish(Geo g, S *__restrict__ b0, S *__restrict__ b1, const S *__restrict__ side_tmp,
@@ -1164,7 +1168,7 @@ template <class S> S *SIDE(const DevLattice &d, int p)
 {
     return static_cast<S *>(d.side) + (size_t)(p & 1) * 9 * (size_t)d.g.nper;
 }
-// Pull scheme only: the scratch slot after the two parities (see k_pull2).
+// Pull scheme only: the scratch slot after the two parities (see k_sweep2).
 template <class S> S *SIDE_TMP(const DevLattice &d)
 {
     return static_cast<S *>(d.side) + 2 * 9 * (size_t)d.g.nper;
@@ -1216,24 +1220,24 @@ void launch_pull(const DevLattice &d, int src, int side_par, bool ghosts, cudaSt
     }
 }
 
-template <class S, int TW, int TH>
-static void launch_pull2_t(const DevLattice &d, int src, int n_par, cudaStream_t s)
+template <class S, int W, int H>
+static void launch_sweep2_t(const DevLattice &d, int src, int n_par, cudaStream_t s)
 {
-    constexpr size_t smem = pull2_smem_bytes<S, TW, TH>();
-    cudaFuncSetAttribute(k_pull2<S, TW, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    dim3 grid(cdiv(d.g.lx, TW), cdiv(d.g.ly, TH));
-    k_pull2<S, TW, TH><<<grid, PULL2_THREADS, smem, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
-                                                      SIDE<S>(d, n_par + 1), SIDE_TMP<S>(d), SIDE<S>(d, n_par),
-                                                      d.scale, d.inv_scale);
+    constexpr size_t smem = sweep2_smem_bytes<S, W>();
+    cudaFuncSetAttribute(k_sweep2<S, W, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 grid(cdiv(d.g.lx, W), cdiv(d.g.ly, H));
+    k_sweep2<S, W, H><<<grid, W, smem, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
+                                         SIDE<S>(d, n_par + 1), SIDE_TMP<S>(d), SIDE<S>(d, n_par), d.scale,
+                                         d.inv_scale);
 }
 
 void launch_pull2(const DevLattice &d, int src, int n_par, cudaStream_t s)
 {
     switch (d.precision) {
-    case LBGPU_F64: launch_pull2_t<double, 32, 16>(d, src, n_par, s); break;
-    case LBGPU_F32: launch_pull2_t<float, 64, 16>(d, src, n_par, s); break;
-    case LBGPU_F16: launch_pull2_t<__half, 64, 16>(d, src, n_par, s); break;
-    default: launch_pull2_t<__nv_bfloat16, 64, 16>(d, src, n_par, s); break;
+    case LBGPU_F64: launch_sweep2_t<double, 128, 128>(d, src, n_par, s); break;
+    case LBGPU_F32: launch_sweep2_t<float, 128, 128>(d, src, n_par, s); break;
+    case LBGPU_F16: launch_sweep2_t<__half, 128, 128>(d, src, n_par, s); break;
+    default: launch_sweep2_t<__nv_bfloat16, 128, 128>(d, src, n_par, s); break;
     }
     const int nthreads = std::max(d.g.nper, d.g.nghost());
     LBGPU_DISPATCH(d, (k_pull2_finish<S><<<cdiv(nthreads, 256), 256, 0, s>>>(d.g, B<S>(d, 0), B<S>(d, 1),

@@ -29,7 +29,7 @@ struct Lattice {
     long long n = 0;     // index of the last collision (form C) or of the state (form L)
     bool ghosts = false; // keep the ghost ring exact (drop-in interface)
     bool zgb_each_step = false;  // native: extrapolated outlet before every step
-    int sweep_steps = 1;         // pull scheme: 2 = two steps per sweep where eligible (k_pull2)
+    int sweep_steps = 1;         // pull scheme: 2 = two steps per sweep where eligible (k_sweep2)
     cudaStream_t stream = nullptr;
     size_t bytes = 0;
     int launches = 0;    // kernels launched by the last public call
