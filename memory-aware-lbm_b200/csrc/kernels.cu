@@ -659,10 +659,15 @@ __device__ __forceinline__ void aa_even_node(const Geo &g, S *__restrict__ a, co
     const bool edge = g.perimeter(X, Y);
     const int p = edge ? g.pidx(X, Y) : 0;
     typename Work<S>::W f[9];
+    if (!edge) {   // the nine loads back to back (a per-slot address choice serialises them)
 #pragma unroll
-    for (int i = 0; i < 9; ++i) {
-        const bool stale = edge && !g.interior(X - cx(i), Y - cy(i));
-        f[i] = Work<S>::load(stale ? side[(size_t)i * g.nper + p] : plane(a, g, i)[o], i, inv);
+        for (int i = 0; i < 9; ++i) f[i] = Work<S>::load(plane(a, g, i)[o], i, inv);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const bool stale = !g.interior(X - cx(i), Y - cy(i));
+            f[i] = Work<S>::load(stale ? side[(size_t)i * g.nper + p] : plane(a, g, i)[o], i, inv);
+        }
     }
     collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
 #pragma unroll
