@@ -650,7 +650,7 @@ __global__ void k_pull2_finish(Geo g, S *__restrict__ b0, S *__restrict__ b1, co
 
 // Even step at node (X, Y): own natural slots (stale ones from the side store) -> collide ->
 // own opposite slots.
-template <class S>
+template <class S, int SH = 2>
 __device__ __forceinline__ void aa_even_node(const Geo &g, S *__restrict__ a, const uint8_t *__restrict__ tag,
                                              const double *__restrict__ bc, double omega,
                                              S *__restrict__ side, float sc, float inv, int X, int Y)
@@ -669,9 +669,9 @@ __device__ __forceinline__ void aa_even_node(const Geo &g, S *__restrict__ a, co
             f[i] = Work<S>::load(stale ? side[(size_t)i * g.nper + p] : plane(a, g, i)[o], i, inv);
         }
     }
-    collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
+    collide_w<S, SH>(bc, g, tag[o], X, Y, f, omega, sc, inv);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) plane(a, g, opp(i))[o] = Work<S>::store(stored_out<S>(g, Y, i, f[i], sc), i, sc);
+    for (int i = 0; i < 9; ++i) plane(a, g, opp(i))[o] = Work<S>::store(stored_out<S, SH>(g, Y, i, f[i], sc), i, sc);
     if (edge) {
 #pragma unroll
         for (int i = 0; i < 9; ++i)
@@ -684,7 +684,7 @@ __device__ __forceinline__ void aa_even_node(const Geo &g, S *__restrict__ a, co
 // natural slot.  Slot A[i][x + c_i] is read (as opp of the neighbour's gather) and written by
 // the same thread, so the in-place update is race-free.  Destinations in the ghost ring are
 // written too, so the natural form carries the values streamed out of the lattice.
-template <class S>
+template <class S, int SH = 2>
 __device__ __forceinline__ void aa_odd_node(const Geo &g, S *__restrict__ a, const uint8_t *__restrict__ tag,
                                             const double *__restrict__ bc, double omega,
                                             S *__restrict__ side, float sc, float inv, int X, int Y)
@@ -705,10 +705,10 @@ __device__ __forceinline__ void aa_odd_node(const Geo &g, S *__restrict__ a, con
                                                     : side[(size_t)i * g.nper + p], i, inv);
         }
     }
-    collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
+    collide_w<S, SH>(bc, g, tag[o], X, Y, f, omega, sc, inv);
 #pragma unroll
     for (int i = 0; i < 9; ++i)
-        plane(a, g, i)[o + cx(i) + (long long)cy(i) * g.pitch] = Work<S>::store(stored_out<S>(g, Y, i, f[i], sc), i, sc);
+        plane(a, g, i)[o + cx(i) + (long long)cy(i) * g.pitch] = Work<S>::store(stored_out<S, SH>(g, Y, i, f[i], sc), i, sc);
     if (edge) {
 #pragma unroll
         for (int i = 0; i < 9; ++i)
@@ -736,6 +736,139 @@ __global__ void __launch_bounds__(BX) k_aa_odd(Geo g, S *__restrict__ a,
     const int X = blockIdx.x * BX + threadIdx.x + 1;
     const int Y = blockIdx.y + 1;
     if (X <= g.lx) aa_odd_node<S>(g, a, tag, bc, omega, side, sc, inv, X, Y);
+}
+
+// AA steps for 16-bit storage, four nodes per thread (the layout of pull_quad: x0 = 1 mod 4,
+// each warp one row of 128 nodes; warps touching the perimeter or the row's end run the
+// per-node functions).  Even step: the quad's natural slots in, its opposite slots out, both
+// aligned.  Odd step: sources gathered as in pull_quad; the scatter to x + c_i shifts the quad by
+// one element, so for c_ix = +-1 the aligned word pair is assembled from the neighbouring lane's
+// value (one shuffle), and the element that belongs to the next (previous) warp is written by
+// its own lane with a 2-byte store.  Every slot is read only by the node whose result is written
+// into it (aa_odd_node), and each lane has consumed its loads before the shuffles that precede
+// the stores, so the in-place update stays race-free.
+template <class S, bool SHIFT>
+__device__ __forceinline__ bool aa_quad_vec(const Geo &g, int x0, int Y, int lane)
+{
+    const int xw0 = x0 - 4 * lane;
+    return (xw0 >= 2) && (xw0 + 127 <= g.lx - 1) && (Y >= 2) && (Y <= g.ly - 1);
+}
+
+template <class S, bool SHIFT>
+__device__ __forceinline__ void aa_collide_quad(const Geo &g, const uint8_t *__restrict__ tag,
+                                                const double *__restrict__ bc, double omega, float sc,
+                                                float inv, int x0, int Y, long long o, float D[4][9])
+{
+    const unsigned tq = *reinterpret_cast<const unsigned *>(tag + o);
+    if (tq == 0x01010101u) {
+        const float om = (float)omega;
+        const float us = SHIFT ? g.shift_u[Y] : 0.0f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) bgk_offsets<SHIFT>(D[k], om, sc, inv, us);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            collide_w<S, SHIFT ? 1 : 0>(bc, g, (int)((tq >> (8 * k)) & 0xff), x0 + k, Y, D[k], omega, sc, inv);
+    }
+    if (SHIFT) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) D[k][i] = stored_out<S, 1>(g, Y, i, D[k][i], sc);
+    }
+}
+
+template <class S, bool SHIFT>
+__global__ void __launch_bounds__(BX, SHIFT ? 7 : 8) k_aa4_even(Geo g, S *__restrict__ a, const uint8_t *__restrict__ tag,
+                                                  const double *__restrict__ bc, double omega,
+                                                  S *__restrict__ side, float sc, float inv)
+{
+    using H = Half2Ops<S>;
+    const int x0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x), Y = blockIdx.y + 1, lane = threadIdx.x & 31;
+    if (!aa_quad_vec<S, SHIFT>(g, x0, Y, lane)) {
+        for (int k = 0; k < 4; ++k)
+            if (x0 + k <= g.lx) aa_even_node<S, SHIFT ? 1 : 0>(g, a, tag, bc, omega, side, sc, inv, x0 + k, Y);
+        return;
+    }
+    const long long o = g.idx(x0, Y);
+    float D[4][9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const uint2 v = *reinterpret_cast<const uint2 *>(plane(a, g, i) + o);
+        D[0][i] = H::lo(v.x); D[1][i] = H::hi(v.x);
+        D[2][i] = H::lo(v.y); D[3][i] = H::hi(v.y);
+    }
+    aa_collide_quad<S, SHIFT>(g, tag, bc, omega, sc, inv, x0, Y, o, D);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        uint2 w;
+        w.x = H::pack(D[0][i], D[1][i]);
+        w.y = H::pack(D[2][i], D[3][i]);
+        *reinterpret_cast<uint2 *>(plane(a, g, opp(i)) + o) = w;
+    }
+}
+
+template <class S, bool SHIFT>
+__global__ void __launch_bounds__(BX, SHIFT ? 6 : 7) k_aa4_odd(Geo g, S *__restrict__ a, const uint8_t *__restrict__ tag,
+                                                 const double *__restrict__ bc, double omega,
+                                                 S *__restrict__ side, float sc, float inv)
+{
+    using H = Half2Ops<S>;
+    const int x0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x), Y = blockIdx.y + 1, lane = threadIdx.x & 31;
+    if (!aa_quad_vec<S, SHIFT>(g, x0, Y, lane)) {
+        for (int k = 0; k < 4; ++k)
+            if (x0 + k <= g.lx) aa_odd_node<S, SHIFT ? 1 : 0>(g, a, tag, bc, omega, side, sc, inv, x0 + k, Y);
+        return;
+    }
+    const long long o = g.idx(x0, Y);
+    float D[4][9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {   // direction i gathered from the opposite slots of x - c_i
+        const S *row = plane(a, g, opp(i)) + (o - (long long)cy(i) * g.pitch);
+        const uint2 v = *reinterpret_cast<const uint2 *>(row);
+        unsigned w0 = v.x, w1 = v.y;
+        if (cx(i) == 1) {            // sources x0-1..x0+2
+            const unsigned e = *reinterpret_cast<const unsigned *>(row - 2);
+            const unsigned n0 = __byte_perm(e, w0, 0x5432), n1 = __byte_perm(w0, w1, 0x5432);
+            w0 = n0; w1 = n1;
+        } else if (cx(i) == -1) {    // sources x0+1..x0+4
+            const unsigned e = *reinterpret_cast<const unsigned *>(row + 4);
+            const unsigned n0 = __byte_perm(w0, w1, 0x5432), n1 = __byte_perm(w1, e, 0x5432);
+            w0 = n0; w1 = n1;
+        }
+        D[0][i] = H::lo(w0); D[1][i] = H::hi(w0);
+        D[2][i] = H::lo(w1); D[3][i] = H::hi(w1);
+    }
+    aa_collide_quad<S, SHIFT>(g, tag, bc, omega, sc, inv, x0, Y, o, D);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {    // direction i scattered to the natural slots of x + c_i
+        const unsigned w0 = H::pack(D[0][i], D[1][i]), w1 = H::pack(D[2][i], D[3][i]);
+        S *drow = plane(a, g, i) + (o + (long long)cy(i) * g.pitch);
+        unsigned short *h = reinterpret_cast<unsigned short *>(drow);
+        if (cx(i) == 0) {
+            *reinterpret_cast<uint2 *>(drow) = make_uint2(w0, w1);
+        } else if (cx(i) == 1) {     // positions x0..x0+3 take nodes x0-1 (previous lane), x0, x0+1, x0+2
+            const unsigned pw = __shfl_up_sync(0xffffffffu, w1, 1);
+            const unsigned n0 = __byte_perm(pw, w0, 0x5432), n1 = __byte_perm(w0, w1, 0x5432);
+            if (lane != 0) {
+                *reinterpret_cast<uint2 *>(drow) = make_uint2(n0, n1);
+            } else {                 // position x0 belongs to the previous warp's last lane
+                h[1] = (unsigned short)(w0 & 0xffffu);
+                *reinterpret_cast<unsigned *>(drow + 2) = n1;
+            }
+            if (lane == 31) h[4] = (unsigned short)(w1 >> 16);
+        } else {                     // positions x0..x0+3 take nodes x0+1, x0+2, x0+3, x0+4 (next lane)
+            const unsigned nw = __shfl_down_sync(0xffffffffu, w0, 1);
+            const unsigned n0 = __byte_perm(w0, w1, 0x5432), n1 = __byte_perm(w1, nw, 0x5432);
+            if (lane != 31) {
+                *reinterpret_cast<uint2 *>(drow) = make_uint2(n0, n1);
+            } else {                 // position x0+3 belongs to the next warp's first lane
+                *reinterpret_cast<unsigned *>(drow) = n0;
+                h[2] = (unsigned short)(w1 >> 16);
+            }
+            if (lane == 0) h[-1] = (unsigned short)(w0 & 0xffffu);
+        }
+    }
 }
 
 // ---- many lattices in one launch ----------------------------------------------------------
@@ -1256,8 +1389,27 @@ void launch_stream(const DevLattice &d, int src, int side_par, cudaStream_t s)
                        SIDE<S>(d, side_par))));
 }
 
+template <class S>
+static void launch_aa4(const DevLattice &d, bool odd, int side_par, cudaStream_t s)
+{
+    dim3 grid(cdiv((d.g.lx + 3) / 4, BX), d.g.ly);
+    if (odd) {
+        if (d.g.shift_u) k_aa4_odd<S, true><<<grid, BX, 0, s>>>(d.g, B<S>(d, 0), d.tag, d.bc, d.omega,
+                                                             SIDE<S>(d, side_par), d.scale, d.inv_scale);
+        else k_aa4_odd<S, false><<<grid, BX, 0, s>>>(d.g, B<S>(d, 0), d.tag, d.bc, d.omega,
+                                                   SIDE<S>(d, side_par), d.scale, d.inv_scale);
+    } else {
+        if (d.g.shift_u) k_aa4_even<S, true><<<grid, BX, 0, s>>>(d.g, B<S>(d, 0), d.tag, d.bc, d.omega,
+                                                              SIDE<S>(d, side_par), d.scale, d.inv_scale);
+        else k_aa4_even<S, false><<<grid, BX, 0, s>>>(d.g, B<S>(d, 0), d.tag, d.bc, d.omega,
+                                                    SIDE<S>(d, side_par), d.scale, d.inv_scale);
+    }
+}
+
 void launch_aa_even(const DevLattice &d, int side_par, cudaStream_t s)
 {
+    if (d.precision == LBGPU_F16) return launch_aa4<__half>(d, false, side_par, s);
+    if (d.precision == LBGPU_BF16) return launch_aa4<__nv_bfloat16>(d, false, side_par, s);
     dim3 grid(cdiv(d.g.lx, BX), d.g.ly);
     LBGPU_DISPATCH(d, (k_aa_even<S><<<grid, BX, 0, s>>>(d.g, B<S>(d, 0), d.tag, d.bc, d.omega,
                        SIDE<S>(d, side_par), d.scale, d.inv_scale)));
@@ -1265,6 +1417,8 @@ void launch_aa_even(const DevLattice &d, int side_par, cudaStream_t s)
 
 void launch_aa_odd(const DevLattice &d, int side_par, cudaStream_t s)
 {
+    if (d.precision == LBGPU_F16) return launch_aa4<__half>(d, true, side_par, s);
+    if (d.precision == LBGPU_BF16) return launch_aa4<__nv_bfloat16>(d, true, side_par, s);
     dim3 grid(cdiv(d.g.lx, BX), d.g.ly);
     LBGPU_DISPATCH(d, (k_aa_odd<S><<<grid, BX, 0, s>>>(d.g, B<S>(d, 0), d.tag, d.bc, d.omega,
                        SIDE<S>(d, side_par), d.scale, d.inv_scale)));
