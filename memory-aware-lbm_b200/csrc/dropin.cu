@@ -59,6 +59,10 @@ struct DropIn {
     uint64_t *dynp_dev = nullptr;
     std::vector<const void *> slot_src;  // [8*nb] boundary data object of each table slot
     std::vector<int> active_slots;
+    // per active slot: the two values' addresses in the driver's data object and their table
+    // offsets (set at each rescan, so a refresh does no index arithmetic)
+    struct SlotRead { const double *src[2]; size_t off[2]; };
+    std::vector<SlotRead> slot_reads;
     std::vector<const double *> omegas;  // distinct omega pointers of bgk / bulk dynamics
     std::vector<double> bc_new;
     const PressureBCData *zgb_base = nullptr;
@@ -143,6 +147,21 @@ int scan_dynamics(Simulation *sim, DropIn *c)
                 }
             }
         }
+    c->slot_reads.clear();
+    for (int k : c->active_slots) {
+        const int tb = k / nb, coord = k % nb;
+        DropIn::SlotRead r;
+        if (tb < 4) {
+            const VelocityBCData *vd = static_cast<const VelocityBCData *>(c->slot_src[k]);
+            r.src[0] = &vd->ux; r.src[1] = &vd->uy;
+        } else {
+            const PressureBCData *pd = static_cast<const PressureBCData *>(c->slot_src[k]);
+            r.src[0] = &pd->rho; r.src[1] = &pd->uPar;
+        }
+        r.off[0] = (size_t)(tb * 2 + 0) * nb + coord;
+        r.off[1] = (size_t)(tb * 2 + 1) * nb + coord;
+        c->slot_reads.push_back(r);
+    }
     c->bc_force = true;
     c->zgb_base = nullptr;
     c->zgb_base_ly = -1;
@@ -153,7 +172,6 @@ int scan_dynamics(Simulation *sim, DropIn *c)
 int refresh_params(DropIn *c)
 {
     Lattice &L = c->L;
-    const int nb = L.d.g.nb;
     if (c->omegas.empty()) {
         L.d.omega = 1.0;
     } else {
@@ -164,21 +182,21 @@ int refresh_params(DropIn *c)
                                  w, *c->omegas[k]);
         L.d.omega = w;
     }
-    c->bc_new = L.bc_host;
-    for (int k : c->active_slots) {
-        const int tb = k / nb, coord = k % nb;
-        double v0, v1;
-        if (tb < 4) {
-            const VelocityBCData *vd = static_cast<const VelocityBCData *>(c->slot_src[k]);
-            v0 = vd->ux; v1 = vd->uy;
-        } else {
-            const PressureBCData *pd = static_cast<const PressureBCData *>(c->slot_src[k]);
-            v0 = pd->rho; v1 = pd->uPar;
+    // bc_new mirrors the last uploaded tables; each active slot is compared with the driver's
+    // object (bitwise, as a memcmp would) and the tables go up only when one changed or a pass
+    // forced it (a rescan, or device-side writes of the two-step outlet)
+    if (c->bc_new.size() != L.bc_host.size()) c->bc_new = L.bc_host;
+    bool changed = c->bc_force;
+    double *bcn = c->bc_new.data();
+    for (const DropIn::SlotRead &r : c->slot_reads)
+        for (int j = 0; j < 2; ++j) {
+            const double v = *r.src[j];
+            if (std::memcmp(&bcn[r.off[j]], &v, sizeof(double)) != 0) {
+                bcn[r.off[j]] = v;
+                changed = true;
+            }
         }
-        c->bc_new[(size_t)(tb * 2 + 0) * nb + coord] = v0;
-        c->bc_new[(size_t)(tb * 2 + 1) * nb + coord] = v1;
-    }
-    if (c->bc_force || std::memcmp(c->bc_new.data(), L.bc_host.data(), c->bc_new.size() * 8) != 0) {
+    if (changed) {
         if (int rc = L.upload_bc(c->bc_new.data())) return rc;
         c->bc_force = false;
     }
@@ -234,8 +252,9 @@ int create_device(Simulation *sim, DropIn *c)
     return LB_OK;
 }
 
-// Bring the device copy up to date before an entry point runs.
-DropIn *prepare(Simulation *sim, const char *fn)
+// Bring the device copy up to date before an entry point runs (`tables`: the entry collides,
+// so omega and the boundary data objects are re-read; a pure stream never reads them).
+DropIn *prepare(Simulation *sim, const char *fn, bool tables = true)
 {
     DropIn *c = ctx_of(sim);
     if (!c) {
@@ -268,7 +287,7 @@ DropIn *prepare(Simulation *sim, const char *fn)
         }
         c->pops_dirty = false;
     }
-    if (refresh_params(c) != LB_OK) return nullptr;
+    if (tables && refresh_params(c) != LB_OK) return nullptr;
     return c;
 }
 
@@ -284,10 +303,9 @@ void finish(Simulation *sim, DropIn *c)
         L.readout_records(reinterpret_cast<double *>(host), 10, c->dynp_dev, 0, sim->lx + 2);
         return;
     }
-    for (int X : {sim->lx - 2, sim->lx - 1}) {
-        if (X < 0 || X > sim->lx + 1) continue;
-        L.readout_records(reinterpret_cast<double *>(host + (size_t)X * col), 10, c->dynp_dev, X, X + 1);
-    }
+    // columns lx-2 and lx-1 are adjacent in the host's y-contiguous node array: one read-out
+    const int X0 = sim->lx >= 2 ? sim->lx - 2 : 0;
+    L.readout_records(reinterpret_cast<double *>(host + (size_t)X0 * col), 10, c->dynp_dev, X0, sim->lx);
 }
 
 void swap_host(Simulation *sim)
@@ -461,7 +479,7 @@ void collide_openmp(Simulation *sim) { collide(sim); }
 
 void propagate(Simulation *sim)
 {
-    DropIn *c = prepare(sim, "propagate");
+    DropIn *c = prepare(sim, "propagate", false);
     if (!c) return;
     c->L.launches = 0;
     c->tmp_is_stream = false;
@@ -491,7 +509,7 @@ void finalize_stream(Simulation *sim)
         swap_host(sim);  // nothing on the device yet: the host arrays are the state
         return;
     }
-    c = prepare(sim, "finalize_stream");
+    c = prepare(sim, "finalize_stream", false);
     if (!c) return;
     Lattice &L = c->L;
     L.launches = 0;
