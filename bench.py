@@ -41,8 +41,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "memory-aware-lbm_b200")
 sys.path.insert(0, PKG)
 
-BYTES_PER_UPDATE = {"f64": 144, "f32": 72, "f16": 36, "bf16": 36,
-                    "f16s": 36, "bf16s": 36}   # "s": 16-bit offsets from the inflow profile per row
+# 16-bit suffixes (lbgpu.storage_form): "s" offsets from the inflow profile per row, "r"
+# stochastic rounding; neither changes the bytes moved
+BYTES_PER_UPDATE = {"f64": 144, "f32": 72, **{p + sfx: 36 for p in ("f16", "bf16")
+                                              for sfx in ("", "s", "r", "sr")}}
 
 
 def parse():
@@ -282,16 +284,12 @@ def run_reference_arm(args, dist):
 # ---------------------------------------------------------------------------------------
 def time_lattice(lbgpu, nx, ny, precision, scheme, steps, warmup, dist, sampler_dev=None):
     ox, oy, r = cylinder(nx, ny)
-    shifted = precision.endswith("s")
-    base = precision[:-1] if shifted else precision
+    base = lbgpu.storage_form(precision)[0]
     lat = lbgpu.Lattice(nx, ny, base, "pull" if scheme == "pull2" else scheme)
     try:
         if scheme == "pull2":
             lat.set_sweep_steps(2)
-        if base in ("f16", "bf16"):   # the scale and shift encode the initial state: set them first
-            lat.set_offset_scale((lbgpu.DEFAULT_SHIFT_SCALE if shifted else lbgpu.DEFAULT_SCALE)[base])
-        if shifted:
-            lat.set_offset_shift(lbgpu.poiseuille_profile(ny, 0.02))
+        lbgpu.configure_storage(lat, precision, 0.02)   # encodes the initial state: set it first
         lat.setup_cylinder(ox, oy, r, 0.02, 100.0, lbgpu.WALL_BOUNCEBACK, lbgpu.OUTLET_CONST)
         lat.step(warmup)
         lat.synchronize()
@@ -334,7 +332,8 @@ def run_ours(args, dist):
     vlist = []
     if args.variants == "auto":
         vlist = [("f64", "aa"), ("f64", "pull2"), ("f32", "pull"), ("f32", "aa"), ("f32", "pull2"),
-                 ("f16", "pull"), ("bf16", "pull"), ("f16", "aa"), ("f16", "pull2")]
+                 ("f16", "pull"), ("bf16", "pull"), ("f16", "aa"), ("f16", "pull2"),
+                 ("f16r", "pull"), ("f16sr", "pull"), ("f16r", "aa")]
     elif args.variants != "none":
         vlist = [tuple(v.split(":")) for v in args.variants.split(",") if v]
     for prec, sch in vlist:

@@ -128,6 +128,16 @@ int lbgpu_set_offset_scale(lbgpu_lattice *lat, int scale_log2);
  * LB_ERR_STATE for FP64/FP32 lattices.  No counterpart in the reference (FP64 only). */
 int lbgpu_set_offset_shift(lbgpu_lattice *lat, const double *u_row);
 
+/* FP16/BF16 storage only: round stored post-collision values stochastically (on = 1) instead
+ * of to nearest (on = 0, the default).  Rounding to nearest drops every change of a stored value
+ * below half its quantum, so a slow transient stalls in 16-bit storage; stochastic rounding keeps
+ * the stored value unbiased (sm_100a hardware conversion `cvt.rs`).  The random bits of a value
+ * are a function of (seed, collision number, node, direction) only: results are deterministic for
+ * a seed and identical across the pull scheme, the AA scheme and two steps per sweep.  Initial
+ * states and uploads still round to nearest.  Lattices with it on step alone (a batch refuses
+ * them, LB_ERR_STATE).  LB_ERR_STATE for FP64/FP32 lattices.  No counterpart in the reference. */
+int lbgpu_set_stochastic_rounding(lbgpu_lattice *lat, int on, unsigned seed);
+
 /* Cylinder channel on the device without host population arrays: tags and tables as the
  * application driver builds them (obstacle disk, walls, Poiseuille inlet, pressure outlet)
  * and equilibrium populations at rho = 1 and the Poiseuille profile.  Returns omega through

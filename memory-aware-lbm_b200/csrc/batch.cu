@@ -307,6 +307,8 @@ int lbgpu_batch_add(lbgpu_batch *b, lbgpu_lattice *lat, int *slot)
                          lat->L.precision, b->precision);
     if (lat->L.zgb_each_step)
         return set_error(LB_ERR_ARG, "lbgpu_batch_add: extrapolated outlets are stepped on their own, not in a batch");
+    if (lat->L.rs)
+        return set_error(LB_ERR_STATE, "lbgpu_batch_add: stochastically rounded lattices step on their own");
     for (lbgpu_lattice *m : b->members)
         if (m == lat) return set_error(LB_ERR_ARG, "lbgpu_batch_add: lattice already in the batch");
     // the member's own stream may still be writing its initial state
@@ -395,6 +397,9 @@ int lbgpu_batch_step(lbgpu_batch *b, int nsteps)
     if (!b || nsteps < 0) return set_error(LB_ERR_ARG, "lbgpu_batch_step: bad arguments");
     b->launches = 0;
     if (nsteps == 0 || lbgpu_batch_size(b) == 0) return LB_OK;
+    for (lbgpu_lattice *m : b->members)
+        if (m && m->L.rs)
+            return set_error(LB_ERR_STATE, "lbgpu_batch_step: a member rounds stochastically (it steps on its own)");
     // A member that needs its first step on its own (see needs_own_step) makes every member
     // take that step on its own path (the same per-node arithmetic as the batch kernel).
     bool own = false;

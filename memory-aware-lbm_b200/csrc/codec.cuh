@@ -55,4 +55,70 @@ template <> struct Codec<__nv_bfloat16> {
     }
 };
 
+// ---- stochastic rounding of 16-bit stores --------------------------------------------------
+//
+// Round to nearest loses every change of a stored value smaller than half its quantum: in a slow
+// transient (a channel building its pressure gradient, a wake drifting) the 16-bit state stalls
+// where the FP64 one moves on.  Stochastic rounding (Croci & Giles, "Effects of round-to-nearest
+// and stochastic rounding in the numerical solution of the heat equation in low precision", 2020)
+// rounds up with probability equal to the discarded fraction, so the stored value is unbiased.
+// sm_100a converts with it in hardware: `cvt.rs.f16x2.f32 d, a, b, rbits` (and `.bf16x2`) adds
+// random bits to the discarded mantissa bits and truncates.  The operand a goes to the upper half
+// of d and takes its random bits from bits 16.. of rbits, b to the lower half with bits 0..
+// (13 bits a value for FP16, 16 for BF16).
+//
+// The random bits of a value depend only on (seed, collision number k, node, direction), so every
+// scheme that produces the same post-collision value stores the same bits:
+//   key_k = rs_key(seed, k)                      per collision (host), never 0
+//   h     = rs_mix((Y (lx + 2) + X) ^ key_k)     per node
+//   r_i   = bits 16..31 of h * K_i               per direction, K_i odd
+// rs_mix is the 32-bit integer hash "lowbias32" (C. Wellons, hash-prospector).
+__host__ __device__ __forceinline__ unsigned rs_mix(unsigned x)
+{
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+__host__ __device__ __forceinline__ unsigned rs_key(unsigned seed, unsigned long long k)
+{
+    const unsigned lo = (unsigned)k, hi = (unsigned)(k >> 32);
+    return rs_mix(seed ^ rs_mix(lo ^ rs_mix(hi + 0x9e3779b9u))) | 1u;
+}
+
+__host__ __device__ __forceinline__ unsigned rs_dir(unsigned h, int i)
+{
+    return h * (0x9e3779b9u * (unsigned)(2 * i + 1));   // odd multiplier: a bijection of h
+}
+
+template <class S> struct RsOps;
+template <> struct RsOps<__half> {
+    // two values (lo -> bits 0..15, hi -> bits 16..31 of the result), random words rlo, rhi
+    static __device__ __forceinline__ unsigned pack(float lo, float hi, unsigned rlo, unsigned rhi)
+    {
+        unsigned d;
+        asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(__byte_perm(rlo, rhi, 0x7632)));
+        return d;
+    }
+    static __device__ __forceinline__ __half one(float v, unsigned r)
+    {
+        return __ushort_as_half((unsigned short)(pack(v, 0.0f, r, 0u) & 0xffffu));
+    }
+};
+template <> struct RsOps<__nv_bfloat16> {
+    static __device__ __forceinline__ unsigned pack(float lo, float hi, unsigned rlo, unsigned rhi)
+    {
+        unsigned d;
+        asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(__byte_perm(rlo, rhi, 0x7632)));
+        return d;
+    }
+    static __device__ __forceinline__ __nv_bfloat16 one(float v, unsigned r)
+    {
+        return __ushort_as_bfloat16((unsigned short)(pack(v, 0.0f, r, 0u) & 0xffffu));
+    }
+};
+
 }  // namespace lbgpu

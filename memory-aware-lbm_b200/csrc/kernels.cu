@@ -199,6 +199,26 @@ template <> struct Work<__nv_bfloat16> {
     static __device__ __forceinline__ __nv_bfloat16 store(float w, int, float) { return __float2bfloat16_rn(w); }
 };
 
+// Stochastic rounding (codec.cuh) is a compile-time choice of a kernel (RS), so no store
+// carries a branch: RS kernels run only for 16-bit lattices with it on, whose collision key is
+// then never 0.
+// The random word of node (X, Y) for a collision key.
+template <class S, bool RS>
+__device__ __forceinline__ unsigned rs_node(const Geo &g, unsigned key, int X, int Y)
+{
+    if constexpr (RS && sizeof(S) == 2) return rs_mix(((unsigned)Y * (unsigned)(g.lx + 2) + (unsigned)X) ^ key);
+    return 0u;
+}
+
+// A post-collision working value of direction i as stored: rounded to nearest, or (RS)
+// stochastically with the node's random word h.
+template <class S, bool RS>
+__device__ __forceinline__ S put(typename Work<S>::W w, int i, float sc, unsigned h)
+{
+    if constexpr (RS && sizeof(S) == 2) return RsOps<S>::one(w, rs_dir(h, i));
+    return Work<S>::store(w, i, sc);
+}
+
 // Decode / encode of a value consumed at row Y (read-outs, uploads, initial states).
 template <class S>
 __device__ __forceinline__ typename Codec<S>::R dec_row(const Geo &g, S v, int i, float inv, int Y)
@@ -295,7 +315,7 @@ __device__ __forceinline__ void collide_w(const double *__restrict__ bc, const G
 
 // In-place collision of every interior node (form L -> form C); the perimeter nodes also
 // record their stale slots' post-collision values in the side parity given.
-template <class S>
+template <class S, bool RS>
 __global__ void __launch_bounds__(BX) k_collide_inplace(Geo g, S *__restrict__ buf,
                                                         const uint8_t *__restrict__ tag,
                                                         const double *__restrict__ bc, double omega,
@@ -311,13 +331,14 @@ __global__ void __launch_bounds__(BX) k_collide_inplace(Geo g, S *__restrict__ b
 #pragma unroll
     for (int i = 0; i < 9; ++i) f[i] = Work<S>::load(plane(buf, g, i)[o], i, inv);
     collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
+    const unsigned h = rs_node<S, RS>(g, g.rs_key, X, Y);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) plane(buf, g, i)[o] = Work<S>::store(stored_out<S>(g, Y, i, f[i], sc), i, sc);
+    for (int i = 0; i < 9; ++i) plane(buf, g, i)[o] = put<S, RS>(stored_out<S>(g, Y, i, f[i], sc), i, sc, h);
     if (g.perimeter(X, Y)) {
         const int p = g.pidx(X, Y);
 #pragma unroll
         for (int i = 0; i < 9; ++i)
-            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
+            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = put<S, RS>(f[i], i, sc, h);
     }
 }
 
@@ -373,11 +394,11 @@ __global__ void __launch_bounds__(BX) k_pull(Geo g, const S *__restrict__ src, S
 }
 
 // Pull step of one node, any storage type (the general path of every pull kernel).
-template <class S, int SH = 2>
+template <class S, int SH = 2, bool RS = false>
 __device__ __forceinline__ void pull_node(const Geo &g, const S *__restrict__ src, S *__restrict__ dst,
                                           const uint8_t *__restrict__ tag, const double *__restrict__ bc,
                                           double omega, S *__restrict__ side, float sc, float inv,
-                                          int X, int Y)
+                                          int X, int Y, unsigned key = 0u)
 {
     const long long o = g.idx(X, Y);
     typename Work<S>::W f[9];
@@ -396,13 +417,38 @@ __device__ __forceinline__ void pull_node(const Geo &g, const S *__restrict__ sr
         }
     }
     collide_w<S, SH>(bc, g, tag[o], X, Y, f, omega, sc, inv);
+    const unsigned h = rs_node<S, RS>(g, key, X, Y);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = Work<S>::store(stored_out<S, SH>(g, Y, i, f[i], sc), i, sc);
+    for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = put<S, RS>(stored_out<S, SH>(g, Y, i, f[i], sc), i, sc, h);
     if (edge) {
 #pragma unroll
         for (int i = 0; i < 9; ++i)
-            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
+            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = put<S, RS>(f[i], i, sc, h);
     }
+}
+
+// Random words of the quad's nodes x0..x0+3 (RS only).
+template <class S, bool RS>
+__device__ __forceinline__ void quad_words(const Geo &g, unsigned key, int x0, int Y, unsigned h[4])
+{
+    const unsigned id = (unsigned)Y * (unsigned)(g.lx + 2) + (unsigned)x0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) h[k] = RS ? rs_mix((id + (unsigned)k) ^ key) : 0u;
+}
+
+// Direction i of a quad's four working values as the stored aligned word pair.
+template <class S, bool RS>
+__device__ __forceinline__ uint2 pack_quad(const float D[4][9], int i, const unsigned h[4])
+{
+    uint2 w;
+    if constexpr (RS) {
+        w.x = RsOps<S>::pack(D[0][i], D[1][i], rs_dir(h[0], i), rs_dir(h[1], i));
+        w.y = RsOps<S>::pack(D[2][i], D[3][i], rs_dir(h[2], i), rs_dir(h[3], i));
+    } else {
+        w.x = Half2Ops<S>::pack(D[0][i], D[1][i]);
+        w.y = Half2Ops<S>::pack(D[2][i], D[3][i]);
+    }
+    return w;
 }
 
 // Pull step for 16-bit storage, four nodes per thread (X = x0..x0+3 with x0 = 1 mod 4, so a
@@ -415,18 +461,18 @@ __device__ __forceinline__ void pull_node(const Geo &g, const S *__restrict__ sr
 //
 // pull_quad runs the four nodes x0..x0+3 of row Y for one lane of a warp whose lanes cover 128
 // consecutive nodes (the choice between the vector and the per-node path is made per warp).
-template <class S, bool SHIFT>
+template <class S, bool SHIFT, bool RS = false>
 __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ src, S *__restrict__ dst,
                                           const uint8_t *__restrict__ tag, const double *__restrict__ bc,
                                           double omega, S *__restrict__ side, float sc, float inv, int x0,
-                                          int Y, int lane)
+                                          int Y, int lane, unsigned key = 0u)
 {
     using H = Half2Ops<S>;
     const int xw0 = x0 - 4 * lane;
     const bool vec = (xw0 >= 2) && (xw0 + 127 <= g.lx - 1) && (Y >= 2) && (Y <= g.ly - 1);
     if (!vec) {
         for (int k = 0; k < 4; ++k)
-            if (x0 + k <= g.lx) pull_node<S, SHIFT ? 1 : 0>(g, src, dst, tag, bc, omega, side, sc, inv, x0 + k, Y);
+            if (x0 + k <= g.lx) pull_node<S, SHIFT ? 1 : 0, RS>(g, src, dst, tag, bc, omega, side, sc, inv, x0 + k, Y, key);
         return;
     }
     const long long o = g.idx(x0, Y);
@@ -466,30 +512,30 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
         for (int k = 0; k < 4; ++k)
             collide_w<S, SHIFT ? 1 : 0>(bc, g, (int)((tq >> (8 * k)) & 0xff), x0 + k, Y, D[k], omega, sc, inv);
     }
+    unsigned h[4];
+    quad_words<S, RS>(g, key, x0, Y, h);
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
         if (SHIFT) {
 #pragma unroll
             for (int k = 0; k < 4; ++k) D[k][i] = stored_out<S, 1>(g, Y, i, D[k][i], sc);
         }
-        uint2 w;
-        w.x = H::pack(D[0][i], D[1][i]);
-        w.y = H::pack(D[2][i], D[3][i]);
-        *reinterpret_cast<uint2 *>(plane(dst, g, i) + o) = w;
+        *reinterpret_cast<uint2 *>(plane(dst, g, i) + o) = pack_quad<S, RS>(D, i, h);
     }
 }
 
 // Eight blocks of 128 threads a SM (64 registers): more loads in flight than the 72-register
 // allocation's seven, for a few bytes of spills on the per-node fallback path.  The shifted form
 // holds the row's rebase values as well and keeps seven (72 registers).
-template <class S, bool SHIFT>
+template <class S, bool SHIFT, bool RS>
 __global__ void __launch_bounds__(BX, SHIFT ? 7 : 8) k_pull4h(Geo g, const S *__restrict__ src, S *__restrict__ dst,
                                                const uint8_t *__restrict__ tag,
                                                const double *__restrict__ bc, double omega,
                                                S *__restrict__ side, float sc, float inv)
 {
     const int t = blockIdx.x * BX + threadIdx.x;
-    pull_quad<S, SHIFT>(g, src, dst, tag, bc, omega, side, sc, inv, 1 + 4 * t, blockIdx.y + 1, threadIdx.x & 31);
+    pull_quad<S, SHIFT, RS>(g, src, dst, tag, bc, omega, side, sc, inv, 1 + 4 * t, blockIdx.y + 1, threadIdx.x & 31,
+                            g.rs_key);
 }
 
 // Propagation of C_n in `src` into `dst` (form C -> form L), ghost ring included; stale
@@ -535,7 +581,7 @@ constexpr size_t sweep2_r0_bytes() { return (3 * 9 * (size_t)(W + 4) * sizeof(S)
 template <class S, int W>
 constexpr size_t sweep2_smem_bytes() { return sweep2_r0_bytes<S, W>() + 3 * 9 * (size_t)(W + 2) * sizeof(S); }
 
-template <class S, int W, int H>
+template <class S, int W, int H, bool RS>
 __global__ void __launch_bounds__(W) k_sweep2(Geo g, const S *__restrict__ src, S *__restrict__ dst,
                                              const uint8_t *__restrict__ tag, const double *__restrict__ bc,
                                              double omega, const S *__restrict__ side_a,
@@ -581,13 +627,14 @@ __global__ void __launch_bounds__(W) k_sweep2(Geo g, const S *__restrict__ src, 
                 }
                 collide_w<S>(bc, g, tag[g.idx(X, Y1)], X, Y1, f, omega, sc, inv);
                 const int sl = (Y1 + 3) % 3;
+                const unsigned h = rs_node<S, RS>(g, g.rs_key, X, Y1);
 #pragma unroll
-                for (int i = 0; i < 9; ++i) r1[sl][i][k] = Work<S>::store(stored_out<S>(g, Y1, i, f[i], sc), i, sc);
+                for (int i = 0; i < 9; ++i) r1[sl][i][k] = put<S, RS>(stored_out<S>(g, Y1, i, f[i], sc), i, sc, h);
                 if (edge && X >= x0 && X < x0 + W && Y1 >= y0 && Y1 < yend) {
 #pragma unroll
                     for (int i = 0; i < 9; ++i)
                         if (!g.interior(X - cx(i), Y1 - cy(i)))
-                            side_tmp[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
+                            side_tmp[(size_t)i * g.nper + p] = put<S, RS>(f[i], i, sc, h);
                 }
             }
         }
@@ -607,12 +654,13 @@ __global__ void __launch_bounds__(W) k_sweep2(Geo g, const S *__restrict__ src, 
             }
             const long long o = g.idx(X, Y2);
             collide_w<S>(bc, g, tag[o], X, Y2, f, omega, sc, inv);
+            const unsigned h = rs_node<S, RS>(g, g.rs_key2, X, Y2);
 #pragma unroll
-            for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = Work<S>::store(stored_out<S>(g, Y2, i, f[i], sc), i, sc);
+            for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = put<S, RS>(stored_out<S>(g, Y2, i, f[i], sc), i, sc, h);
             if (edge) {
 #pragma unroll
                 for (int i = 0; i < 9; ++i)
-                    if (!g.interior(X - cx(i), Y2 - cy(i))) side_b[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
+                    if (!g.interior(X - cx(i), Y2 - cy(i))) side_b[(size_t)i * g.nper + p] = put<S, RS>(f[i], i, sc, h);
             }
         }
     }
@@ -650,10 +698,10 @@ __global__ void k_pull2_finish(Geo g, S *__restrict__ b0, S *__restrict__ b1, co
 
 // Even step at node (X, Y): own natural slots (stale ones from the side store) -> collide ->
 // own opposite slots.
-template <class S, int SH = 2>
+template <class S, int SH = 2, bool RS = false>
 __device__ __forceinline__ void aa_even_node(const Geo &g, S *__restrict__ a, const uint8_t *__restrict__ tag,
                                              const double *__restrict__ bc, double omega,
-                                             S *__restrict__ side, float sc, float inv, int X, int Y)
+                                             S *__restrict__ side, float sc, float inv, int X, int Y, unsigned key = 0u)
 {
     const long long o = g.idx(X, Y);
     const bool edge = g.perimeter(X, Y);
@@ -670,12 +718,13 @@ __device__ __forceinline__ void aa_even_node(const Geo &g, S *__restrict__ a, co
         }
     }
     collide_w<S, SH>(bc, g, tag[o], X, Y, f, omega, sc, inv);
+    const unsigned h = rs_node<S, RS>(g, key, X, Y);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) plane(a, g, opp(i))[o] = Work<S>::store(stored_out<S, SH>(g, Y, i, f[i], sc), i, sc);
+    for (int i = 0; i < 9; ++i) plane(a, g, opp(i))[o] = put<S, RS>(stored_out<S, SH>(g, Y, i, f[i], sc), i, sc, h);
     if (edge) {
 #pragma unroll
         for (int i = 0; i < 9; ++i)
-            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
+            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = put<S, RS>(f[i], i, sc, h);
     }
 }
 
@@ -684,10 +733,10 @@ __device__ __forceinline__ void aa_even_node(const Geo &g, S *__restrict__ a, co
 // natural slot.  Slot A[i][x + c_i] is read (as opp of the neighbour's gather) and written by
 // the same thread, so the in-place update is race-free.  Destinations in the ghost ring are
 // written too, so the natural form carries the values streamed out of the lattice.
-template <class S, int SH = 2>
+template <class S, int SH = 2, bool RS = false>
 __device__ __forceinline__ void aa_odd_node(const Geo &g, S *__restrict__ a, const uint8_t *__restrict__ tag,
                                             const double *__restrict__ bc, double omega,
-                                            S *__restrict__ side, float sc, float inv, int X, int Y)
+                                            S *__restrict__ side, float sc, float inv, int X, int Y, unsigned key = 0u)
 {
     const long long o = g.idx(X, Y);
     const bool edge = g.perimeter(X, Y);
@@ -706,13 +755,14 @@ __device__ __forceinline__ void aa_odd_node(const Geo &g, S *__restrict__ a, con
         }
     }
     collide_w<S, SH>(bc, g, tag[o], X, Y, f, omega, sc, inv);
+    const unsigned h = rs_node<S, RS>(g, key, X, Y);
 #pragma unroll
     for (int i = 0; i < 9; ++i)
-        plane(a, g, i)[o + cx(i) + (long long)cy(i) * g.pitch] = Work<S>::store(stored_out<S, SH>(g, Y, i, f[i], sc), i, sc);
+        plane(a, g, i)[o + cx(i) + (long long)cy(i) * g.pitch] = put<S, RS>(stored_out<S, SH>(g, Y, i, f[i], sc), i, sc, h);
     if (edge) {
 #pragma unroll
         for (int i = 0; i < 9; ++i)
-            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = Work<S>::store(f[i], i, sc);
+            if (!g.interior(X - cx(i), Y - cy(i))) side[(size_t)i * g.nper + p] = put<S, RS>(f[i], i, sc, h);
     }
 }
 
@@ -778,16 +828,17 @@ __device__ __forceinline__ void aa_collide_quad(const Geo &g, const uint8_t *__r
     }
 }
 
-template <class S, bool SHIFT>
+template <class S, bool SHIFT, bool RS>
 __global__ void __launch_bounds__(BX, SHIFT ? 7 : 8) k_aa4_even(Geo g, S *__restrict__ a, const uint8_t *__restrict__ tag,
                                                   const double *__restrict__ bc, double omega,
                                                   S *__restrict__ side, float sc, float inv)
 {
     using H = Half2Ops<S>;
     const int x0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x), Y = blockIdx.y + 1, lane = threadIdx.x & 31;
+    const unsigned key = g.rs_key;
     if (!aa_quad_vec<S, SHIFT>(g, x0, Y, lane)) {
         for (int k = 0; k < 4; ++k)
-            if (x0 + k <= g.lx) aa_even_node<S, SHIFT ? 1 : 0>(g, a, tag, bc, omega, side, sc, inv, x0 + k, Y);
+            if (x0 + k <= g.lx) aa_even_node<S, SHIFT ? 1 : 0, RS>(g, a, tag, bc, omega, side, sc, inv, x0 + k, Y, key);
         return;
     }
     const long long o = g.idx(x0, Y);
@@ -799,25 +850,23 @@ __global__ void __launch_bounds__(BX, SHIFT ? 7 : 8) k_aa4_even(Geo g, S *__rest
         D[2][i] = H::lo(v.y); D[3][i] = H::hi(v.y);
     }
     aa_collide_quad<S, SHIFT>(g, tag, bc, omega, sc, inv, x0, Y, o, D);
+    unsigned h[4];
+    quad_words<S, RS>(g, key, x0, Y, h);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) {
-        uint2 w;
-        w.x = H::pack(D[0][i], D[1][i]);
-        w.y = H::pack(D[2][i], D[3][i]);
-        *reinterpret_cast<uint2 *>(plane(a, g, opp(i)) + o) = w;
-    }
+    for (int i = 0; i < 9; ++i) *reinterpret_cast<uint2 *>(plane(a, g, opp(i)) + o) = pack_quad<S, RS>(D, i, h);
 }
 
-template <class S, bool SHIFT>
+template <class S, bool SHIFT, bool RS>
 __global__ void __launch_bounds__(BX, SHIFT ? 6 : 7) k_aa4_odd(Geo g, S *__restrict__ a, const uint8_t *__restrict__ tag,
                                                  const double *__restrict__ bc, double omega,
                                                  S *__restrict__ side, float sc, float inv)
 {
     using H = Half2Ops<S>;
     const int x0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x), Y = blockIdx.y + 1, lane = threadIdx.x & 31;
+    const unsigned key = g.rs_key;
     if (!aa_quad_vec<S, SHIFT>(g, x0, Y, lane)) {
         for (int k = 0; k < 4; ++k)
-            if (x0 + k <= g.lx) aa_odd_node<S, SHIFT ? 1 : 0>(g, a, tag, bc, omega, side, sc, inv, x0 + k, Y);
+            if (x0 + k <= g.lx) aa_odd_node<S, SHIFT ? 1 : 0, RS>(g, a, tag, bc, omega, side, sc, inv, x0 + k, Y, key);
         return;
     }
     const long long o = g.idx(x0, Y);
@@ -840,9 +889,12 @@ __global__ void __launch_bounds__(BX, SHIFT ? 6 : 7) k_aa4_odd(Geo g, S *__restr
         D[2][i] = H::lo(w1); D[3][i] = H::hi(w1);
     }
     aa_collide_quad<S, SHIFT>(g, tag, bc, omega, sc, inv, x0, Y, o, D);
+    unsigned hw[4];
+    quad_words<S, RS>(g, key, x0, Y, hw);
 #pragma unroll
     for (int i = 0; i < 9; ++i) {    // direction i scattered to the natural slots of x + c_i
-        const unsigned w0 = H::pack(D[0][i], D[1][i]), w1 = H::pack(D[2][i], D[3][i]);
+        const uint2 wq = pack_quad<S, RS>(D, i, hw);
+        const unsigned w0 = wq.x, w1 = wq.y;
         S *drow = plane(a, g, i) + (o + (long long)cy(i) * g.pitch);
         unsigned short *h = reinterpret_cast<unsigned short *>(drow);
         if (cx(i) == 0) {
@@ -1326,19 +1378,35 @@ template <class S> S *SIDE_TMP(const DevLattice &d)
 void launch_collide_inplace(const DevLattice &d, int cur, int side_par, cudaStream_t s)
 {
     dim3 grid(cdiv(d.g.lx, BX), d.g.ly);
-    LBGPU_DISPATCH(d, (k_collide_inplace<S><<<grid, BX, 0, s>>>(d.g, B<S>(d, cur), d.tag, d.bc,
-                       d.omega, SIDE<S>(d, side_par), d.scale, d.inv_scale)));
+    if (d.g.rs_key && d.precision == LBGPU_F16)
+        k_collide_inplace<__half, true><<<grid, BX, 0, s>>>(d.g, B<__half>(d, cur), d.tag, d.bc, d.omega,
+                                                           SIDE<__half>(d, side_par), d.scale, d.inv_scale);
+    else if (d.g.rs_key && d.precision == LBGPU_BF16)
+        k_collide_inplace<__nv_bfloat16, true><<<grid, BX, 0, s>>>(d.g, B<__nv_bfloat16>(d, cur), d.tag, d.bc,
+                                                                  d.omega, SIDE<__nv_bfloat16>(d, side_par),
+                                                                  d.scale, d.inv_scale);
+    else
+        LBGPU_DISPATCH(d, (k_collide_inplace<S, false><<<grid, BX, 0, s>>>(d.g, B<S>(d, cur), d.tag, d.bc,
+                           d.omega, SIDE<S>(d, side_par), d.scale, d.inv_scale)));
+}
+
+template <class S, bool SHIFT, bool RS>
+static void launch_pull4h_t(const DevLattice &d, dim3 grid, int src, int side_par, cudaStream_t s)
+{
+    k_pull4h<S, SHIFT, RS><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
+                                               SIDE<S>(d, side_par), d.scale, d.inv_scale);
 }
 
 template <class S>
 static void launch_pull4h(const DevLattice &d, dim3 grid, int src, int side_par, cudaStream_t s)
 {
-    if (d.g.shift_u)
-        k_pull4h<S, true><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
-                                              SIDE<S>(d, side_par), d.scale, d.inv_scale);
-    else
-        k_pull4h<S, false><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
-                                               SIDE<S>(d, side_par), d.scale, d.inv_scale);
+    if (d.g.shift_u) {
+        if (d.g.rs_key) launch_pull4h_t<S, true, true>(d, grid, src, side_par, s);
+        else launch_pull4h_t<S, true, false>(d, grid, src, side_par, s);
+    } else {
+        if (d.g.rs_key) launch_pull4h_t<S, false, true>(d, grid, src, side_par, s);
+        else launch_pull4h_t<S, false, false>(d, grid, src, side_par, s);
+    }
 }
 
 void launch_pull(const DevLattice &d, int src, int side_par, bool ghosts, cudaStream_t s)
@@ -1358,13 +1426,13 @@ void launch_pull(const DevLattice &d, int src, int side_par, bool ghosts, cudaSt
     }
 }
 
-template <class S, int W, int H>
+template <class S, int W, int H, bool RS = false>
 static void launch_sweep2_t(const DevLattice &d, int src, int n_par, cudaStream_t s)
 {
     constexpr size_t smem = sweep2_smem_bytes<S, W>();
-    cudaFuncSetAttribute(k_sweep2<S, W, H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_sweep2<S, W, H, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid(cdiv(d.g.lx, W), cdiv(d.g.ly, H));
-    k_sweep2<S, W, H><<<grid, W, smem, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
+    k_sweep2<S, W, H, RS><<<grid, W, smem, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
                                          SIDE<S>(d, n_par + 1), SIDE_TMP<S>(d), SIDE<S>(d, n_par), d.scale,
                                          d.inv_scale);
 }
@@ -1374,8 +1442,14 @@ void launch_pull2(const DevLattice &d, int src, int n_par, cudaStream_t s)
     switch (d.precision) {
     case LBGPU_F64: launch_sweep2_t<double, 128, 128>(d, src, n_par, s); break;
     case LBGPU_F32: launch_sweep2_t<float, 128, 128>(d, src, n_par, s); break;
-    case LBGPU_F16: launch_sweep2_t<__half, 128, 128>(d, src, n_par, s); break;
-    default: launch_sweep2_t<__nv_bfloat16, 128, 128>(d, src, n_par, s); break;
+    case LBGPU_F16:
+        if (d.g.rs_key) launch_sweep2_t<__half, 128, 128, true>(d, src, n_par, s);
+        else launch_sweep2_t<__half, 128, 128>(d, src, n_par, s);
+        break;
+    default:
+        if (d.g.rs_key) launch_sweep2_t<__nv_bfloat16, 128, 128, true>(d, src, n_par, s);
+        else launch_sweep2_t<__nv_bfloat16, 128, 128>(d, src, n_par, s);
+        break;
     }
     const int nthreads = std::max(d.g.nper, d.g.nghost());
     LBGPU_DISPATCH(d, (k_pull2_finish<S><<<cdiv(nthreads, 256), 256, 0, s>>>(d.g, B<S>(d, 0), B<S>(d, 1),
@@ -1389,20 +1463,27 @@ void launch_stream(const DevLattice &d, int src, int side_par, cudaStream_t s)
                        SIDE<S>(d, side_par))));
 }
 
+template <class S, bool SHIFT, bool RS>
+static void launch_aa4_t(const DevLattice &d, bool odd, int side_par, cudaStream_t s)
+{
+    dim3 grid(cdiv((d.g.lx + 3) / 4, BX), d.g.ly);
+    if (odd)
+        k_aa4_odd<S, SHIFT, RS><<<grid, BX, 0, s>>>(d.g, B<S>(d, 0), d.tag, d.bc, d.omega,
+                                                    SIDE<S>(d, side_par), d.scale, d.inv_scale);
+    else
+        k_aa4_even<S, SHIFT, RS><<<grid, BX, 0, s>>>(d.g, B<S>(d, 0), d.tag, d.bc, d.omega,
+                                                     SIDE<S>(d, side_par), d.scale, d.inv_scale);
+}
+
 template <class S>
 static void launch_aa4(const DevLattice &d, bool odd, int side_par, cudaStream_t s)
 {
-    dim3 grid(cdiv((d.g.lx + 3) / 4, BX), d.g.ly);
-    if (odd) {
-        if (d.g.shift_u) k_aa4_odd<S, true><<<grid, BX, 0, s>>>(d.g, B<S>(d, 0), d.tag, d.bc, d.omega,
-                                                             SIDE<S>(d, side_par), d.scale, d.inv_scale);
-        else k_aa4_odd<S, false><<<grid, BX, 0, s>>>(d.g, B<S>(d, 0), d.tag, d.bc, d.omega,
-                                                   SIDE<S>(d, side_par), d.scale, d.inv_scale);
+    if (d.g.shift_u) {
+        if (d.g.rs_key) launch_aa4_t<S, true, true>(d, odd, side_par, s);
+        else launch_aa4_t<S, true, false>(d, odd, side_par, s);
     } else {
-        if (d.g.shift_u) k_aa4_even<S, true><<<grid, BX, 0, s>>>(d.g, B<S>(d, 0), d.tag, d.bc, d.omega,
-                                                              SIDE<S>(d, side_par), d.scale, d.inv_scale);
-        else k_aa4_even<S, false><<<grid, BX, 0, s>>>(d.g, B<S>(d, 0), d.tag, d.bc, d.omega,
-                                                    SIDE<S>(d, side_par), d.scale, d.inv_scale);
+        if (d.g.rs_key) launch_aa4_t<S, false, true>(d, odd, side_par, s);
+        else launch_aa4_t<S, false, false>(d, odd, side_par, s);
     }
 }
 

@@ -3,6 +3,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include "codec.cuh"
 #include "lattice.h"
 #include "lbgpu.h"
 
@@ -154,15 +155,24 @@ void Lattice::view(int &v, int &par) const
     v = (form == FORM_C && pending) ? VIEW_PULL_PENDING : VIEW_DIRECT;
 }
 
+// Collision k produces the post-collision state C_k; its stored values round with key k.
+void Lattice::set_rs_keys(long long k)
+{
+    d.g.rs_key = rs ? rs_key(rs_seed, (unsigned long long)k) : 0u;
+    d.g.rs_key2 = rs ? rs_key(rs_seed, (unsigned long long)(k + 1)) : 0u;
+}
+
 // ---- state machine (pull scheme) ------------------------------------------------------
 int Lattice::op_collide()
 {
     if (scheme != LBGPU_PULL) return set_error(LB_ERR_STATE, "collide/propagate need the pull scheme");
     if (form == FORM_C && pending) {
+        set_rs_keys(n + 1);
         launch_pull(d, cur, (int)((n + 1) & 1), ghosts, stream);
         cur = 1 - cur;
         ++n;
     } else {
+        set_rs_keys(n);
         launch_collide_inplace(d, cur, (int)(n & 1), stream);
         form = FORM_C;
     }
@@ -219,10 +229,12 @@ int Lattice::zgb_pass()
 int Lattice::aa_step()
 {
     if (form == FORM_L) {
+        set_rs_keys(n);
         launch_aa_even(d, (int)(n & 1), stream);
         form = FORM_C;
         pending = 1;
     } else {
+        set_rs_keys(n + 1);
         launch_aa_odd(d, (int)((n + 1) & 1), stream);
         n += 2;
         form = FORM_L;
@@ -242,6 +254,7 @@ int Lattice::step(int nsteps)
             LB_TRY(aa_step());
         } else if (sweep_steps == 2 && nsteps - s >= 2 && !zgb_each_step && !ghosts && form == FORM_C && pending) {
             // two steps in one sweep: C_n -> C_{n+2} in the other buffer, still pending
+            set_rs_keys(n + 1);
             launch_pull2(d, cur, (int)(n & 1), stream);
             launches += 2;
             cur = 1 - cur;

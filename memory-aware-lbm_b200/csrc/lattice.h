@@ -69,6 +69,10 @@ struct Lattice {
     double *red_scratch = nullptr;  // (ly+2)*8 partial sums + 8 results
     double *vel_acc = nullptr;      // 2*lx*ly running velocity sums
     float *shift = nullptr;         // 16-bit storage: per-row shift velocity [ly+2] (d.g.shift_u)
+    bool rs = false;                // 16-bit storage: stochastic rounding of stored values
+    unsigned rs_seed = 0;
+    // the keys of collision k (and k + 1, two-step sweep) into d.g before a collision launch
+    void set_rs_keys(long long k);
     long long vel_samples = 0;
     int check(const char *what);   // cudaGetLastError -> error code
     int side_par_stale() const { return (int)((n + 1) & 1); }

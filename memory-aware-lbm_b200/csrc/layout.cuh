@@ -30,6 +30,9 @@ struct Geo {
     // w_i.  Layout, all float, Y = 0..ly+1: u_s[Y]; base[Y][9] = S_i(Y); rebase[Y][9] =
     // S_i(Y) - S_i(Y + c_iy) (0 where c_iy = 0 or the row is a ghost row).
     const float *shift_u;
+    // 16-bit storage only: stochastic rounding keys (codec.cuh) of the launch's collision and,
+    // for the two-step sweep, of the second one; 0 rounds to nearest.
+    unsigned rs_key, rs_key2;
     __host__ __device__ __forceinline__ const float *shift_base(int Y) const { return shift_u + (ly + 2) + 9 * Y; }
     __host__ __device__ __forceinline__ const float *shift_rebase(int Y) const
     {
@@ -80,6 +83,8 @@ inline Geo make_geo(int lx, int ly, int elem_bytes)
     g.nb = (lx > ly ? lx : ly) + 2;
     g.nper = 2 * lx + 2 * ly;
     g.shift_u = nullptr;
+    g.rs_key = 0;
+    g.rs_key2 = 0;
     return g;
 }
 

@@ -171,6 +171,20 @@ int lbgpu_set_offset_shift(lbgpu_lattice *h, const double *u_row)
     return LB_OK;
 }
 
+int lbgpu_set_stochastic_rounding(lbgpu_lattice *h, int on, unsigned seed)
+{
+    if (int rc = bad_handle(h, "lbgpu_set_stochastic_rounding")) return rc;
+    Lattice &L = h->L;
+    if (L.precision != LBGPU_F16 && L.precision != LBGPU_BF16)
+        return set_error(LB_ERR_STATE, "lbgpu_set_stochastic_rounding: FP16/BF16 storage only");
+    if (on != 0 && on != 1) return set_error(LB_ERR_ARG, "lbgpu_set_stochastic_rounding: on = %d", on);
+    L.rs = on != 0;
+    L.rs_seed = seed;
+    L.d.g.rs_key = 0;
+    L.d.g.rs_key2 = 0;
+    return LB_OK;
+}
+
 int lbgpu_set_populations(lbgpu_lattice *h, const double *f, const double *tmp)
 {
     if (int rc = bad_handle(h, "lbgpu_set_populations")) return rc;

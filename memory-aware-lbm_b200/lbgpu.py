@@ -83,6 +83,7 @@ def lib():
     L.lbgpu_set_populations.argtypes = [_vp, _dp, _dp]
     L.lbgpu_set_offset_scale.argtypes = [_vp, ctypes.c_int]
     L.lbgpu_set_offset_shift.argtypes = [_vp, _dp]
+    L.lbgpu_set_stochastic_rounding.argtypes = [_vp, ctypes.c_int, ctypes.c_uint]
     L.lbgpu_setup_cylinder.argtypes = [_vp] + [ctypes.c_int] * 3 + [ctypes.c_double] * 2 + [
         ctypes.c_int] * 2 + [_dp]
     L.lbgpu_build_cylinder.restype = ctypes.c_double
@@ -239,6 +240,10 @@ class Lattice:
             raise ValueError(f"shift profile needs {self.ly + 2} values")
         _check(lib().lbgpu_set_offset_shift(self.h, _p(u)))
 
+    def set_stochastic_rounding(self, on=True, seed=0):
+        """FP16/BF16 storage: round stored values stochastically (seeded, deterministic)."""
+        _check(lib().lbgpu_set_stochastic_rounding(self.h, 1 if on else 0, int(seed) & 0xffffffff))
+
     def setup_cylinder(self, obst_x, obst_y, obst_r, umax=0.02, re=100.0, wall=WALL_REGULARIZED,
                        outlet=OUTLET_ZGB):
         om = ctypes.c_double()
@@ -332,6 +337,30 @@ def poiseuille_profile(ly, umax):
     y = np.arange(ly, dtype=np.float64)
     u[1:ly + 1] = 4.0 * umax / (L * L) * (L * y - y * y)
     return u
+
+
+def storage_form(name):
+    """Storage names: 'f64', 'f32', 'f16', 'bf16', and for the 16-bit types the suffixes 's'
+    (offsets from the channel's inflow-profile equilibrium per row, lbgpu_set_offset_shift) and
+    'r' (stochastic rounding, lbgpu_set_stochastic_rounding), e.g. 'f16sr'.
+    Returns (precision, shift, stochastic)."""
+    import re
+    m = re.fullmatch(r"(f64|f32|f16|bf16)(s?)(r?)", name)
+    if not m or (m.group(1) in ("f64", "f32") and (m.group(2) or m.group(3))):
+        raise ValueError(f"storage {name!r}")
+    return m.group(1), bool(m.group(2)), bool(m.group(3))
+
+
+def configure_storage(lat, name, umax, seed=0):
+    """Offset scale, row shift (the inflow profile of peak umax) and rounding of a storage name,
+    applied before the initial state is written."""
+    base, shift, rs = storage_form(name)
+    if base in DEFAULT_SCALE:
+        lat.set_offset_scale((DEFAULT_SHIFT_SCALE if shift else DEFAULT_SCALE)[base])
+    if shift:
+        lat.set_offset_shift(poiseuille_profile(lat.ly, umax))
+    if rs:
+        lat.set_stochastic_rounding(True, seed)
 
 
 def cylinder_lattice(lx, ly, precision="f64", scheme="pull", umax=0.02, re=100.0,

@@ -229,16 +229,11 @@ def serving_study(precisions=("f32", "f16"), n=120, seed=20260102, budget_gb=150
 # ------------------------------------------------------------------------------------------
 # precision
 # ------------------------------------------------------------------------------------------
-def _storage(name):
-    """'f16s' / 'bf16s': 16-bit offsets from the channel's Poiseuille profile (row shift)."""
-    return (name[:-1], True) if name.endswith("s") else (name, False)
-
-
 def _run_averaged(nx, ny, prec, umax, re, steps, avg_every, moment_every):
     ox, oy, r = nx // 5 + 1, ny // 2 + 1, ny // 10 + 1
-    q = dict(lx=nx, ly=ny, obst_x=ox, obst_y=oy, obst_r=r, umax=umax, re=re)
-    base, shifted = _storage(prec)
-    with _channel(q, base, "pull", lbgpu.poiseuille_profile(ny, umax) if shifted else None) as lat:
+    with lbgpu.Lattice(nx, ny, lbgpu.storage_form(prec)[0], "pull") as lat:
+        lbgpu.configure_storage(lat, prec, umax, seed=20260101)
+        lat.setup_cylinder(ox, oy, r, umax, re, lbgpu.WALL_BOUNCEBACK, lbgpu.OUTLET_CONST)
         m0 = lat.moments()
         half = steps // 2
         ms = lat.step_timed(half)
@@ -264,7 +259,8 @@ def _run_averaged(nx, ny, prec, umax, re, steps, avg_every, moment_every):
 
 
 def precision_study(nx=16384, ny=4096, steps=20000, cases=((100.0, 0.02), (1000.0, 0.05)),
-                    precisions=("f16", "bf16", "f16s", "bf16s"), avg_every=10, moment_every=100):
+                    precisions=("f16", "bf16", "f16s", "bf16s", "f16r", "bf16r", "f16sr", "bf16sr"),
+                    avg_every=10, moment_every=100):
     out = {"nx": nx, "ny": ny, "steps": steps, "average": f"every {avg_every} steps over the "
            f"second half", "forces": f"momentum exchange every {moment_every} steps over the "
            "second half; C = F / (0.5 rho U^2 D), U = 2/3 uMax, D = 2r", "cases": []}
@@ -285,10 +281,11 @@ def precision_study(nx=16384, ny=4096, steps=20000, cases=((100.0, 0.02), (1000.
                           "cd_rel_err": abs(r["cd"] - ref["cd"]) / abs(ref["cd"]),
                           "cl_abs_err": abs(r["cl"] - ref["cl"]),
                           "non_finite": r["non_finite"],
-                          "scale_log2": (lbgpu.DEFAULT_SHIFT_SCALE if _storage(prec)[1]
-                                         else lbgpu.DEFAULT_SCALE)[_storage(prec)[0]],
-                          "offsets_from": "Poiseuille-profile equilibrium per row" if _storage(prec)[1]
-                          else "w_i"}
+                          "scale_log2": (lbgpu.DEFAULT_SHIFT_SCALE if lbgpu.storage_form(prec)[1]
+                                         else lbgpu.DEFAULT_SCALE)[lbgpu.storage_form(prec)[0]],
+                          "offsets_from": "Poiseuille-profile equilibrium per row"
+                          if lbgpu.storage_form(prec)[1] else "w_i",
+                          "rounding": "stochastic" if lbgpu.storage_form(prec)[2] else "nearest"}
             del r
         out["cases"].append(case)
         del ref

@@ -16,6 +16,8 @@ from contextlib import redirect_stdout
 import pytest
 import torch.multiprocessing as mp
 
+import lbgpu
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
@@ -31,6 +33,7 @@ class _FakeLattice:
     calls = []
 
     def __init__(self, nx, ny, precision, scheme):
+        self.lx, self.ly = nx, ny
         self.last_launches = 7
         _FakeLattice.calls.append(("new", nx, ny, precision, scheme))
 
@@ -61,14 +64,11 @@ class _FakeLattice:
 
 
 class _FakeLbgpu:
+    """The lbgpu module with the stand-in lattice (its storage helpers are the real ones)."""
     Lattice = _FakeLattice
     WALL_BOUNCEBACK, OUTLET_CONST = 0, 1
-    DEFAULT_SCALE = {"f16": 10, "bf16": 6}
-    DEFAULT_SHIFT_SCALE = {"f16": 17, "bf16": 6}
-
-    @staticmethod
-    def poiseuille_profile(ly, umax):
-        return [0.0] * (ly + 2)
+    storage_form = staticmethod(lbgpu.storage_form)
+    configure_storage = staticmethod(lbgpu.configure_storage)
 
 
 def _rank_main(rank, world, port, out_dir):
@@ -142,6 +142,7 @@ def test_time_lattice_sets_the_lattice_up_in_order(two_ranks):
     new = two_ranks[0]["calls"][0]
     assert new[1:] == [200, 50, "f16", "pull"]
     assert two_ranks[0]["calls"][2] == ["scale", 17]
+    assert two_ranks[0]["calls"][3] == ["shift", 52]
     assert two_ranks[0]["calls"][5] == ["step", 3]
     assert two_ranks[0]["calls"][6] == ["timed", 12]
 
