@@ -99,15 +99,18 @@ int scan_dynamics(Simulation *sim, DropIn *c)
 {
     Lattice &L = c->L;
     const int lx = sim->lx, ly = sim->ly, nb = L.d.g.nb;
-    std::vector<uint8_t> plane((size_t)L.d.g.plane, 0);
+    // tags in the host's own node order (sequential reads and writes; the device transposes)
+    std::vector<uint8_t> txy((size_t)(lx + 2) * (ly + 2), 0);
     c->slot_src.assign(8 * (size_t)nb, nullptr);
     c->active_slots.clear();
     c->omegas.clear();
     const Dynamics *last = nullptr;
     int last_tag = 0;
-    for (int X = 1; X <= lx; ++X)
+    for (int X = 1; X <= lx; ++X) {
+        const uint64_t *col = c->dynp.data() + (size_t)X * (ly + 2);
+        uint8_t *tcol = txy.data() + (size_t)X * (ly + 2);
         for (int Y = 1; Y <= ly; ++Y) {
-            const Dynamics *dyn = reinterpret_cast<const Dynamics *>(c->dynp[(size_t)X * (ly + 2) + Y]);
+            const Dynamics *dyn = reinterpret_cast<const Dynamics *>(col[Y]);
             if (!dyn)
                 return set_error(LB_ERR_DYNAMICS, "node (%d,%d) has no dynamics (setDynamics was not called)", X, Y);
             if (dyn != last) {
@@ -131,7 +134,7 @@ int scan_dynamics(Simulation *sim, DropIn *c)
                 last = dyn;
                 last_tag = t;
             }
-            plane[(size_t)L.d.g.idx(X, Y)] = (uint8_t)last_tag;
+            tcol[Y] = (uint8_t)last_tag;
             if (last_tag >= LBGPU_TAG_UPPER_ZOUHE) {
                 const int tb = lbgpu::tag_table(last_tag);
                 const int coord = (lbgpu::tag_side(last_tag) <= lbgpu::SIDE_LOWER) ? X : Y;
@@ -147,6 +150,7 @@ int scan_dynamics(Simulation *sim, DropIn *c)
                 }
             }
         }
+    }
     c->slot_reads.clear();
     for (int k : c->active_slots) {
         const int tb = k / nb, coord = k % nb;
@@ -165,7 +169,7 @@ int scan_dynamics(Simulation *sim, DropIn *c)
     c->bc_force = true;
     c->zgb_base = nullptr;
     c->zgb_base_ly = -1;
-    return L.upload_tag_plane(plane.data());
+    return L.upload_tags_xy(txy.data());
 }
 
 // Re-read boundary data and omega from the driver's objects; upload what changed.
@@ -270,7 +274,7 @@ DropIn *prepare(Simulation *sim, const char *fn, bool tables = true)
     if (!c->uploaded) {
         L.launches = 0;
         if (L.upload_records(0, reinterpret_cast<const double *>(chunk_of(sim->lattice)), 10, 0, sim->lx + 2) ||
-            L.upload_records(1, reinterpret_cast<const double *>(chunk_of(sim->tmpLattice)), 10, 0, sim->lx + 2) ||
+            L.upload_records_edges(1, reinterpret_cast<const double *>(chunk_of(sim->tmpLattice)), 10) ||
             L.init_side_from(1, 1))
             return nullptr;
         L.cur = 0; L.form = lbgpu::FORM_L; L.pending = 0; L.n = 0;

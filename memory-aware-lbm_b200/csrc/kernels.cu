@@ -346,7 +346,20 @@ __global__ void __launch_bounds__(BX) k_collide_inplace(Geo g, S *__restrict__ b
 // gathers L_{n+1} from its neighbours (stale slots from the side parity holding C_{n-1}),
 // collides, writes C_{n+1} and refreshes the same side parity.  With GHOSTS, ghost-ring nodes
 // of `dst` receive the values streamed out of the lattice, as the reference's propagation
-// writes them (lb.c:258-267).
+// writes them (lb.c:258-267).  Lanes map X = 1, 2, ... as without the ring, so every warp's
+// rows start on a 128-byte line; the thread of column lx+1 also takes ghost column 0.
+template <class S>
+__device__ __forceinline__ void ring_node(const Geo &g, const S *__restrict__ src, S *__restrict__ dst, int X,
+                                          int Y)
+{
+    const long long o = g.idx(X, Y);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const int sx = X - cx(i), sy = Y - cy(i);
+        if (g.interior(sx, sy)) plane(dst, g, i)[o] = plane(src, g, i)[g.idx(sx, sy)];
+    }
+}
+
 template <class S, bool GHOSTS>
 __global__ void __launch_bounds__(BX) k_pull(Geo g, const S *__restrict__ src, S *__restrict__ dst,
                                              const uint8_t *__restrict__ tag,
@@ -355,16 +368,13 @@ __global__ void __launch_bounds__(BX) k_pull(Geo g, const S *__restrict__ src, S
 {
     using C = Codec<S>;
     using R = typename C::R;
-    const int X = blockIdx.x * BX + threadIdx.x + (GHOSTS ? 0 : 1);
+    const int X = blockIdx.x * BX + threadIdx.x + 1;
     const int Y = blockIdx.y + (GHOSTS ? 0 : 1);
     if (X > g.lx + (GHOSTS ? 1 : 0)) return;
     const long long o = g.idx(X, Y);
     if (GHOSTS && !g.interior(X, Y)) {
-#pragma unroll
-        for (int i = 0; i < 9; ++i) {
-            const int sx = X - cx(i), sy = Y - cy(i);
-            if (g.interior(sx, sy)) plane(dst, g, i)[o] = plane(src, g, i)[g.idx(sx, sy)];
-        }
+        ring_node(g, src, dst, X, Y);
+        if (X == g.lx + 1) ring_node(g, src, dst, 0, Y);
         return;
     }
     typename Work<S>::W f[9];
@@ -1064,12 +1074,12 @@ __global__ void __launch_bounds__(BX) k_readout(Geo g, int view, const S *__rest
 // FP64 node records of columns [X0, X1) into buffer b (inverse of k_readout).
 template <class S>
 __global__ void __launch_bounds__(BX) k_upload(Geo g, const double *__restrict__ in, int rs, int X0,
-                                               int X1, S *__restrict__ buf, float sc)
+                                               int X1, int Y0, int H, S *__restrict__ buf, float sc)
 {
-    const int Y = blockIdx.x * BX + threadIdx.x;
+    const int Y = Y0 + blockIdx.x * BX + threadIdx.x;
     const int X = X0 + blockIdx.y;
-    if (Y > g.ly + 1 || X >= X1) return;
-    const size_t r = ((size_t)(X - X0) * (g.ly + 2) + Y) * rs;
+    if (Y >= Y0 + H || X >= X1) return;
+    const size_t r = ((size_t)(X - X0) * H + (Y - Y0)) * rs;
     const long long o = g.idx(X, Y);
 #pragma unroll
     for (int i = 0; i < 9; ++i)
@@ -1412,7 +1422,7 @@ static void launch_pull4h(const DevLattice &d, dim3 grid, int src, int side_par,
 void launch_pull(const DevLattice &d, int src, int side_par, bool ghosts, cudaStream_t s)
 {
     if (ghosts) {
-        dim3 grid(cdiv(d.g.lx + 2, BX), d.g.ly + 2);
+        dim3 grid(cdiv(d.g.lx + 1, BX), d.g.ly + 2);
         LBGPU_DISPATCH(d, (k_pull<S, true><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src),
                            d.tag, d.bc, d.omega, SIDE<S>(d, side_par), d.scale, d.inv_scale)));
     } else if (d.precision == LBGPU_F16 || d.precision == LBGPU_BF16) {
@@ -1597,12 +1607,38 @@ void launch_readout(const DevLattice &d, int view, int cur, int side_par, int X0
 }
 
 void launch_upload(const DevLattice &d, int b, const double *in, int rec_stride, int X0, int X1,
-                   cudaStream_t s)
+                   int Y0, int H, cudaStream_t s)
 {
-    if (X1 <= X0) return;
-    dim3 grid(cdiv(d.g.ly + 2, BX), X1 - X0);
-    LBGPU_DISPATCH(d, (k_upload<S><<<grid, BX, 0, s>>>(d.g, in, rec_stride, X0, X1, B<S>(d, b),
+    if (X1 <= X0 || H <= 0) return;
+    dim3 grid(cdiv(H, BX), X1 - X0);
+    LBGPU_DISPATCH(d, (k_upload<S><<<grid, BX, 0, s>>>(d.g, in, rec_stride, X0, X1, Y0, H, B<S>(d, b),
                        d.scale)));
+}
+
+// Tag plane from a host-order array tag_xy[X * (ly + 2) + Y] (ghost ring included): 32 x 32
+// tiles through shared memory, read along y and written along x.
+__global__ void k_tags_from_xy(Geo g, const uint8_t *__restrict__ in, uint8_t *__restrict__ tag)
+{
+    __shared__ uint8_t t[32][33];
+    const int Y0 = blockIdx.x * 32, X0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+    for (int j = 0; j < 32; j += 8) {
+        const int X = X0 + ty + j, Y = Y0 + tx;
+        if (X < g.lx + 2 && Y < g.ly + 2) t[ty + j][tx] = in[(size_t)X * (g.ly + 2) + Y];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 32; j += 8) {
+        const int Y = Y0 + ty + j, X = X0 + tx;
+        if (X < g.lx + 2 && Y < g.ly + 2) tag[g.idx(X, Y)] = t[tx][ty + j];
+    }
+}
+
+void launch_tags_from_xy(const DevLattice &d, const uint8_t *in, cudaStream_t s)
+{
+    dim3 grid(cdiv(d.g.ly + 2, 32), cdiv(d.g.lx + 2, 32));
+    k_tags_from_xy<<<grid, dim3(32, 8), 0, s>>>(d.g, in, const_cast<uint8_t *>(d.tag));
 }
 
 void launch_zgb_rho(const DevLattice &d, int view, int cur, int side_par, cudaStream_t s)

@@ -40,8 +40,12 @@ void launch_side_from_buf(const DevLattice &d, int b, int side_par, cudaStream_t
 void launch_ghost_copy(const DevLattice &d, int b, cudaStream_t s);
 void launch_readout(const DevLattice &d, int view, int cur, int side_par, int X0, int X1,
                     double *out, int rec_stride, const uint64_t *dynp, cudaStream_t s);
+// Records of columns X0..X1-1, rows Y0..Y0+H-1 (in: [X - X0][Y - Y0][rec_stride] doubles) into
+// buffer b.
 void launch_upload(const DevLattice &d, int b, const double *in, int rec_stride, int X0, int X1,
-                   cudaStream_t s);
+                   int Y0, int H, cudaStream_t s);
+// Tag plane from a device copy of a host-order tag array tag_xy[X * (ly + 2) + Y].
+void launch_tags_from_xy(const DevLattice &d, const uint8_t *in, cudaStream_t s);
 void launch_zgb_rho(const DevLattice &d, int view, int cur, int side_par, cudaStream_t s);
 void launch_zgb_apply(const DevLattice &d, cudaStream_t s);
 void launch_periodic(const DevLattice &d, int b, cudaStream_t s);

@@ -306,10 +306,39 @@ int Lattice::upload_records(int b, const double *host, int rs, int X0, int X1)
         LB_CUDA(cudaMemcpyAsync(stage, host + (size_t)(c0 - X0) * col,
                                 (size_t)(c1 - c0) * col * sizeof(double),
                                 cudaMemcpyHostToDevice, stream), "upload populations");
-        launch_upload(d, b, stage, rs, c0, c1, stream);
+        launch_upload(d, b, stage, rs, c0, c1, 0, ly + 2, stream);
         ++launches;
     }
     return check("upload");
+}
+
+int Lattice::upload_record_rows(int b, const double *host, int rs, int X0, int X1, int Y0, int H)
+{
+    if (X1 <= X0 || H <= 0) return LB_OK;
+    const size_t col = (size_t)(ly + 2) * rs, band = (size_t)H * rs;
+    size_t cols = ((size_t)64 << 20) / (band * sizeof(double));
+    if (cols < 1) cols = 1;
+    if (cols > (size_t)(X1 - X0)) cols = (size_t)(X1 - X0);
+    LB_TRY(ensure_stage(cols * band * sizeof(double)));
+    for (int c0 = X0; c0 < X1; c0 += (int)cols) {
+        const int c1 = (c0 + (int)cols < X1) ? c0 + (int)cols : X1;
+        LB_CUDA(cudaMemcpy2DAsync(stage, band * sizeof(double), host + (size_t)(c0 - X0) * col + (size_t)Y0 * rs,
+                                  col * sizeof(double), band * sizeof(double), (size_t)(c1 - c0),
+                                  cudaMemcpyHostToDevice, stream), "upload population rows");
+        launch_upload(d, b, stage, rs, c0, c1, Y0, H, stream);
+        ++launches;
+    }
+    return check("upload rows");
+}
+
+int Lattice::upload_records_edges(int b, const double *host, int rs)
+{
+    if (lx < 4 || ly < 4) return upload_records(b, host, rs, 0, lx + 2);
+    const size_t col = (size_t)(ly + 2) * rs;
+    LB_TRY(upload_records(b, host, rs, 0, 2));
+    LB_TRY(upload_records(b, host + (size_t)lx * col, rs, lx, lx + 2));
+    LB_TRY(upload_record_rows(b, host + 2 * col, rs, 2, lx, 0, 2));
+    return upload_record_rows(b, host + 2 * col, rs, 2, lx, ly, 2);
 }
 
 int Lattice::readout_records(double *host, int rs, const uint64_t *dynp_dev, int X0, int X1)
@@ -443,7 +472,6 @@ int Lattice::upload_tag_plane(const uint8_t *plane)
 
 int Lattice::upload_tags(const uint8_t *tag_xy)
 {
-    std::vector<uint8_t> plane((size_t)d.g.plane, 0);
     for (int X = 0; X < lx + 2; ++X)
         for (int Y = 0; Y < ly + 2; ++Y) {
             const int t = tag_xy[(size_t)X * (ly + 2) + Y];
@@ -451,9 +479,21 @@ int Lattice::upload_tags(const uint8_t *tag_xy)
                 return set_error(LB_ERR_ARG, "tag %d at (%d,%d) out of range", t, X, Y);
             if (d.g.interior(X, Y) && t == LBGPU_TAG_NONE)
                 return set_error(LB_ERR_DYNAMICS, "interior node (%d,%d) has no dynamics", X, Y);
-            plane[(size_t)d.g.idx(X, Y)] = (uint8_t)t;
         }
-    return upload_tag_plane(plane.data());
+    return upload_tags_xy(tag_xy);
+}
+
+// The host array in its own order to the device, transposed there (a host transpose writes one
+// byte a cache line).
+int Lattice::upload_tags_xy(const uint8_t *tag_xy)
+{
+    const size_t n = (size_t)(lx + 2) * (ly + 2);
+    LB_TRY(ensure_stage(n));
+    LB_CUDA(cudaMemcpyAsync(stage, tag_xy, n, cudaMemcpyHostToDevice, stream), "upload tags");
+    launch_tags_from_xy(d, reinterpret_cast<const uint8_t *>(stage), stream);
+    LB_TRY(check("tags"));
+    LB_CUDA(cudaStreamSynchronize(stream), "upload tags");
+    return LB_OK;
 }
 
 }  // namespace lbgpu

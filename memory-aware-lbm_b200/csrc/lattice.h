@@ -56,9 +56,16 @@ struct Lattice {
     // data movement
     int upload_bc(const double *bc);      // host [16*nb]
     int upload_zgb_src(const int *src);   // host [4*nb]
-    int upload_tags(const uint8_t *tag_xy);  // host tag[X*(ly+2)+Y]
+    int upload_tags(const uint8_t *tag_xy);  // host tag[X*(ly+2)+Y], validated here
     int upload_tag_plane(const uint8_t *plane);  // host plane in device layout
     int upload_records(int b, const double *host, int rs, int X0, int X1);
+    // rows Y0..Y0+H-1 of columns X0..X1-1 from host records laid out like upload_records' (host
+    // points at column X0, row 0)
+    int upload_record_rows(int b, const double *host, int rs, int X0, int X1, int Y0, int H);
+    // the stale-slot and ghost-ring sources of buffer b only: columns 0, 1, lx, lx+1 and rows
+    // 0, 1, ly, ly+1 (the pull kernel writes the rest before anything reads it)
+    int upload_records_edges(int b, const double *host, int rs);
+    int upload_tags_xy(const uint8_t *tag_xy);   // host order, already validated
     int readout_records(double *host, int rs, const uint64_t *dynp_dev, int X0, int X1);
     int init_side_from(int b, int par);
     int init_cylinder(double umax);  // equilibrium Poiseuille populations into buffer 0
