@@ -63,6 +63,7 @@ struct lbgpu_batch {
     cudaEvent_t order = nullptr;             // orders the batch stream against members' streams
     cudaGraphExec_t graph[2] = {nullptr, nullptr};   // one chunk, by aa_phase
     int launches = 0;
+    bool rs = false;                         // some member rounds stochastically (set at rebuild)
 };
 
 namespace {
@@ -92,7 +93,23 @@ BatchInst describe(const Lattice &L)
         b.phase0 = (L.form == lbgpu::FORM_L) ? 0 : 1;
         b.tau0 = (int)((L.form == lbgpu::FORM_L) ? L.n : L.n + 1);
     }
+    b.rs = L.rs ? 1 : 0;
+    b.rs_seed = L.rs_seed;
     return b;
+}
+
+// Stochastically rounded members key their collisions by number (tau0 + k), which a replayed
+// chunk cannot advance: before each chunk after the first of a call the descriptors are
+// uploaded again with tau0 moved on by the steps done (an even number: parities unchanged).
+int refresh_collision_numbers(lbgpu_batch *b, int done)
+{
+    for (size_t i = 0; i < b->members.size(); ++i)
+        if (b->members[i]) {
+            b->h_inst[i] = describe(b->members[i]->L);
+            b->h_inst[i].tau0 += done;
+        }
+    return batch_error(cudaMemcpyAsync(b->d_inst, b->h_inst.data(), b->h_inst.size() * sizeof(BatchInst),
+                                       cudaMemcpyHostToDevice, b->stream), "update batch collision numbers");
 }
 
 // A member's host-side state after `m` batch steps (no launches).
@@ -162,6 +179,8 @@ int rebuild(lbgpu_batch *b)
             for (int x0 = 1; x0 <= L.lx; x0 += tw) work[s].push_back(BatchWork{(int)i, x0, y0, sh});
     }
     b->aa_phase = 0;
+    b->rs = false;
+    for (const BatchInst &d : b->h_inst) b->rs = b->rs || d.rs;
     int need[kLists];
     for (int s = 0; s < kLists; ++s) need[s] = (int)work[s].size();
     if (int rc = ensure_capacity(b, (int)std::max<size_t>(b->h_inst.size(), 1), need)) return rc;
@@ -203,8 +222,8 @@ void launch_step(lbgpu_batch *b, int k)
         }
         const int t = b->threads == 512 ? 2 : (b->threads == 256 ? 1 : 0);
         const int grid = b->persistent ? std::min(b->per_sm[kind][t] * b->sms, b->nwork[s]) : b->nwork[s];
-        lbgpu::launch_batch(b->precision, kind, b->threads, b->persistent, b->d_inst, b->d_work[s], b->nwork[s],
-                            grid, k, b->stream);
+        lbgpu::launch_batch(b->precision, kind, b->threads, b->persistent, b->rs, b->d_inst, b->d_work[s],
+                            b->nwork[s], grid, k, b->stream);
         ++b->launches;
     }
 }
@@ -307,8 +326,6 @@ int lbgpu_batch_add(lbgpu_batch *b, lbgpu_lattice *lat, int *slot)
                          lat->L.precision, b->precision);
     if (lat->L.zgb_each_step)
         return set_error(LB_ERR_ARG, "lbgpu_batch_add: extrapolated outlets are stepped on their own, not in a batch");
-    if (lat->L.rs)
-        return set_error(LB_ERR_STATE, "lbgpu_batch_add: stochastically rounded lattices step on their own");
     for (lbgpu_lattice *m : b->members)
         if (m == lat) return set_error(LB_ERR_ARG, "lbgpu_batch_add: lattice already in the batch");
     // the member's own stream may still be writing its initial state
@@ -397,9 +414,9 @@ int lbgpu_batch_step(lbgpu_batch *b, int nsteps)
     if (!b || nsteps < 0) return set_error(LB_ERR_ARG, "lbgpu_batch_step: bad arguments");
     b->launches = 0;
     if (nsteps == 0 || lbgpu_batch_size(b) == 0) return LB_OK;
+    bool any_rs = false;
     for (lbgpu_lattice *m : b->members)
-        if (m && m->L.rs)
-            return set_error(LB_ERR_STATE, "lbgpu_batch_step: a member rounds stochastically (it steps on its own)");
+        if (m && m->L.rs) any_rs = true;
     // A member that needs its first step on its own (see needs_own_step) makes every member
     // take that step on its own path (the same per-node arithmetic as the batch kernel).
     bool own = false;
@@ -417,11 +434,18 @@ int lbgpu_batch_step(lbgpu_batch *b, int nsteps)
         --nsteps;
         b->dirty = true;
     }
+    // rounding switched (or reseeded) on a member since the descriptors were written
+    for (size_t i = 0; i < b->members.size() && !b->dirty; ++i)
+        if (b->members[i] && (i >= b->h_inst.size() || b->h_inst[i].rs != (b->members[i]->L.rs ? 1 : 0) ||
+                              b->h_inst[i].rs_seed != b->members[i]->L.rs_seed))
+            b->dirty = true;
     if (b->dirty)
         if (int rc = rebuild(b)) return rc;
     if (int rc = order_before(b)) return rc;
     int done = 0;
     while (nsteps - done >= kChunk) {
+        if (any_rs && done)
+            if (int rc = refresh_collision_numbers(b, done)) return rc;
         if (!b->graph[b->aa_phase])
             if (int rc = capture_chunk(b)) return rc;
         if (int rc = batch_error(cudaGraphLaunch(b->graph[b->aa_phase], b->stream), "graph launch")) return rc;
@@ -429,15 +453,18 @@ int lbgpu_batch_step(lbgpu_batch *b, int nsteps)
         done += kChunk;
     }
     const int rem = nsteps - done;
+    if (any_rs && done && rem)
+        if (int rc = refresh_collision_numbers(b, done)) return rc;
     for (int k = 0; k < rem; ++k) launch_step(b, k);
     if (int rc = lbgpu::cuda_error(cudaGetLastError(), "batch step")) return rc;
     for (lbgpu_lattice *m : b->members)
         if (m) advance(m->L, nsteps);
     if (int rc = order_after(b)) return rc;
-    if (rem & 1) {
-        // parities changed: new descriptors before the next call (a chunk's graph reads them),
-        // and the AA lists swap their kind of step
-        b->aa_phase ^= 1;
+    if ((rem & 1) || any_rs) {
+        // parities changed (or stochastically rounded members count collisions): new
+        // descriptors before the next call (a chunk's graph reads them); on odd remainders the
+        // AA lists swap their kind of step
+        if (rem & 1) b->aa_phase ^= 1;
         for (size_t i = 0; i < b->members.size(); ++i)
             if (b->members[i]) b->h_inst[i] = describe(b->members[i]->L);
         if (int rc = batch_error(cudaMemcpyAsync(b->d_inst, b->h_inst.data(), b->h_inst.size() * sizeof(BatchInst),

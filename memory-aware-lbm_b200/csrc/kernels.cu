@@ -964,7 +964,9 @@ constexpr int batch_min_blocks()
     return b128 * 128 / BT > 0 ? b128 * 128 / BT : 1;
 }
 
-template <class S, int KIND, int BT>
+// RS: the kernel also serves stochastically rounded members (16-bit only); batches without
+// any keep kernels without that code, whose registers it would otherwise raise.
+template <class S, int KIND, int BT, bool RS>
 __device__ __forceinline__ void batch_node(const BatchInst *__restrict__ insts, const BatchWork it, int k)
 {
     const BatchInst &d = insts[it.inst];
@@ -977,12 +979,20 @@ __device__ __forceinline__ void batch_node(const BatchInst *__restrict__ insts, 
             const int lane = threadIdx.x & 31;
             S *side = static_cast<S *>(d.side) + (size_t)((d.tau0 + k) & 1) * 9 * (size_t)g.nper;
             const int src = d.cur0 ^ (k & 1);
-            if (g.shift_u)
-                pull_quad<S, true>(g, static_cast<const S *>(d.buf[src]), static_cast<S *>(d.buf[src ^ 1]),
-                                   d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, it.x0 + 4 * lane, Y, lane);
-            else
-                pull_quad<S, false>(g, static_cast<const S *>(d.buf[src]), static_cast<S *>(d.buf[src ^ 1]),
-                                    d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, it.x0 + 4 * lane, Y, lane);
+            const S *sb = static_cast<const S *>(d.buf[src]);
+            S *db = static_cast<S *>(d.buf[src ^ 1]);
+            const int x0 = it.x0 + 4 * lane;
+            if (RS && d.rs) {
+                const unsigned key = rs_key(d.rs_seed, (unsigned long long)(d.tau0 + k));
+                if (g.shift_u)
+                    pull_quad<S, true, true>(g, sb, db, d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, x0, Y, lane, key);
+                else
+                    pull_quad<S, false, true>(g, sb, db, d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, x0, Y, lane, key);
+            } else if (g.shift_u) {
+                pull_quad<S, true>(g, sb, db, d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, x0, Y, lane);
+            } else {
+                pull_quad<S, false>(g, sb, db, d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, x0, Y, lane);
+            }
         }
         return;
     }
@@ -991,6 +1001,23 @@ __device__ __forceinline__ void batch_node(const BatchInst *__restrict__ insts, 
     const int Y = it.y0 + (int)(threadIdx.x >> lw);
     if (X > g.lx || Y > g.ly) return;
     S *side = static_cast<S *>(d.side) + (size_t)((d.tau0 + k) & 1) * 9 * (size_t)g.nper;
+    if constexpr (RS && sizeof(S) == 2) {
+        if (d.rs) {   // the single-lattice arithmetic with the member's collision key
+            const unsigned key = rs_key(d.rs_seed, (unsigned long long)(d.tau0 + k));
+            if (KIND == BATCH_PULL) {
+                const int src = d.cur0 ^ (k & 1);
+                pull_node<S, 2, true>(g, static_cast<const S *>(d.buf[src]), static_cast<S *>(d.buf[src ^ 1]),
+                                      d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, X, Y, key);
+            } else if (KIND == BATCH_AA_EVEN) {
+                aa_even_node<S, 2, true>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, d.omega, side, d.scale,
+                                         d.inv_scale, X, Y, key);
+            } else {
+                aa_odd_node<S, 2, true>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, d.omega, side, d.scale,
+                                        d.inv_scale, X, Y, key);
+            }
+            return;
+        }
+    }
     if (KIND == BATCH_PULL) {
         const int src = d.cur0 ^ (k & 1);
         pull_node<S>(g, static_cast<const S *>(d.buf[src]), static_cast<S *>(d.buf[src ^ 1]), d.tag,
@@ -1004,14 +1031,14 @@ __device__ __forceinline__ void batch_node(const BatchInst *__restrict__ insts, 
     }
 }
 
-template <class S, int KIND, bool PERSIST, int BT>
+template <class S, int KIND, bool PERSIST, int BT, bool RS = false>
 __global__ void __launch_bounds__(BT, (batch_min_blocks<S, KIND, PERSIST, BT>()))
     k_batch(const BatchInst *__restrict__ insts, const BatchWork *__restrict__ work, int nwork, int k)
 {
     if (PERSIST) {
-        for (int w = blockIdx.x; w < nwork; w += gridDim.x) batch_node<S, KIND, BT>(insts, work[w], k);
+        for (int w = blockIdx.x; w < nwork; w += gridDim.x) batch_node<S, KIND, BT, RS>(insts, work[w], k);
     } else if ((int)blockIdx.x < nwork) {
-        batch_node<S, KIND, BT>(insts, work[blockIdx.x], k);
+        batch_node<S, KIND, BT, RS>(insts, work[blockIdx.x], k);
     }
 }
 
@@ -1515,41 +1542,54 @@ void launch_aa_odd(const DevLattice &d, int side_par, cudaStream_t s)
                        SIDE<S>(d, side_par), d.scale, d.inv_scale)));
 }
 
-template <class S, int KIND, int BT>
-static void launch_batch_b(bool persistent, const BatchInst *insts, const BatchWork *work, int nwork, int grid,
+template <class S, int KIND, int BT, bool RS>
+static void launch_batch_r(bool persistent, const BatchInst *insts, const BatchWork *work, int nwork, int grid,
                            int k, cudaStream_t s)
 {
-    if (persistent) k_batch<S, KIND, true, BT><<<grid, BT, 0, s>>>(insts, work, nwork, k);
-    else k_batch<S, KIND, false, BT><<<grid, BT, 0, s>>>(insts, work, nwork, k);
+    if (persistent) k_batch<S, KIND, true, BT, RS><<<grid, BT, 0, s>>>(insts, work, nwork, k);
+    else k_batch<S, KIND, false, BT, RS><<<grid, BT, 0, s>>>(insts, work, nwork, k);
+}
+
+template <class S, int KIND, int BT>
+static void launch_batch_b(bool persistent, bool rs, const BatchInst *insts, const BatchWork *work, int nwork,
+                           int grid, int k, cudaStream_t s)
+{
+    if constexpr (sizeof(S) == 2) {
+        if (rs) return launch_batch_r<S, KIND, BT, true>(persistent, insts, work, nwork, grid, k, s);
+    }
+    launch_batch_r<S, KIND, BT, false>(persistent, insts, work, nwork, grid, k, s);
 }
 
 template <class S, int KIND>
-static void launch_batch_k(int bt, bool persistent, const BatchInst *insts, const BatchWork *work, int nwork,
-                           int grid, int k, cudaStream_t s)
+static void launch_batch_k(int bt, bool persistent, bool rs, const BatchInst *insts, const BatchWork *work,
+                           int nwork, int grid, int k, cudaStream_t s)
 {
-    if (bt == 512) launch_batch_b<S, KIND, 512>(persistent, insts, work, nwork, grid, k, s);
-    else if (bt == 256) launch_batch_b<S, KIND, 256>(persistent, insts, work, nwork, grid, k, s);
-    else launch_batch_b<S, KIND, 128>(persistent, insts, work, nwork, grid, k, s);
+    if (bt == 512) launch_batch_b<S, KIND, 512>(persistent, rs, insts, work, nwork, grid, k, s);
+    else if (bt == 256) launch_batch_b<S, KIND, 256>(persistent, rs, insts, work, nwork, grid, k, s);
+    else launch_batch_b<S, KIND, 128>(persistent, rs, insts, work, nwork, grid, k, s);
 }
 
 template <class S>
-static void launch_batch_t(int kind, int bt, bool persistent, const BatchInst *insts, const BatchWork *work,
-                           int nwork, int grid, int k, cudaStream_t s)
+static void launch_batch_t(int kind, int bt, bool persistent, bool rs, const BatchInst *insts,
+                           const BatchWork *work, int nwork, int grid, int k, cudaStream_t s)
 {
-    if (kind == BATCH_PULL) launch_batch_k<S, BATCH_PULL>(bt, persistent, insts, work, nwork, grid, k, s);
-    else if (kind == BATCH_AA_EVEN) launch_batch_k<S, BATCH_AA_EVEN>(bt, persistent, insts, work, nwork, grid, k, s);
-    else if (kind == BATCH_AA_ODD) launch_batch_k<S, BATCH_AA_ODD>(bt, persistent, insts, work, nwork, grid, k, s);
-    else if constexpr (sizeof(S) == 2) launch_batch_k<S, BATCH_PULL4>(bt, persistent, insts, work, nwork, grid, k, s);
+    if (kind == BATCH_PULL) launch_batch_k<S, BATCH_PULL>(bt, persistent, rs, insts, work, nwork, grid, k, s);
+    else if (kind == BATCH_AA_EVEN)
+        launch_batch_k<S, BATCH_AA_EVEN>(bt, persistent, rs, insts, work, nwork, grid, k, s);
+    else if (kind == BATCH_AA_ODD)
+        launch_batch_k<S, BATCH_AA_ODD>(bt, persistent, rs, insts, work, nwork, grid, k, s);
+    else if constexpr (sizeof(S) == 2)
+        launch_batch_k<S, BATCH_PULL4>(bt, persistent, rs, insts, work, nwork, grid, k, s);
 }
 
-void launch_batch(int precision, int kind, int threads, bool persistent, const BatchInst *insts,
+void launch_batch(int precision, int kind, int threads, bool persistent, bool rs, const BatchInst *insts,
                   const BatchWork *work, int nwork, int grid, int k, cudaStream_t s)
 {
     switch (precision) {
-    case LBGPU_F64: launch_batch_t<double>(kind, threads, persistent, insts, work, nwork, grid, k, s); break;
-    case LBGPU_F32: launch_batch_t<float>(kind, threads, persistent, insts, work, nwork, grid, k, s); break;
-    case LBGPU_F16: launch_batch_t<__half>(kind, threads, persistent, insts, work, nwork, grid, k, s); break;
-    default: launch_batch_t<__nv_bfloat16>(kind, threads, persistent, insts, work, nwork, grid, k, s); break;
+    case LBGPU_F64: launch_batch_t<double>(kind, threads, persistent, false, insts, work, nwork, grid, k, s); break;
+    case LBGPU_F32: launch_batch_t<float>(kind, threads, persistent, false, insts, work, nwork, grid, k, s); break;
+    case LBGPU_F16: launch_batch_t<__half>(kind, threads, persistent, rs, insts, work, nwork, grid, k, s); break;
+    default: launch_batch_t<__nv_bfloat16>(kind, threads, persistent, rs, insts, work, nwork, grid, k, s); break;
     }
 }
 

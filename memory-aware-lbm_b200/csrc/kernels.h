@@ -83,7 +83,9 @@ struct BatchInst {
     const double *bc;
     double omega;
     float scale, inv_scale;
-    int scheme, cur0, phase0, tau0;
+    int scheme, cur0, phase0, tau0;   // tau0 + k: the collision number of step k of a chunk
+    unsigned rs_seed;                 // 16-bit members: stochastic rounding seed (rs != 0)
+    int rs;
 };
 
 // A tile of a lattice: nodes x0 .. x0 + (32 << shape) - 1 and y0 .. y0 + threads / (32 << shape) - 1
@@ -95,7 +97,8 @@ struct BatchWork {
 // Step k of a chunk, of kind BATCH_PULL / AA_EVEN / AA_ODD / PULL4 (16-bit only), for every tile of a
 // work list of `nwork` tiles of `threads` nodes: `persistent` grids of `grid` blocks stride
 // through the list, otherwise `grid` must equal nwork (one block per tile).
-void launch_batch(int precision, int kind, int threads, bool persistent, const BatchInst *insts,
+// rs: some member rounds stochastically (16-bit batches; the kernels then carry that path).
+void launch_batch(int precision, int kind, int threads, bool persistent, bool rs, const BatchInst *insts,
                   const BatchWork *work, int nwork, int grid, int k, cudaStream_t s);
 // Resident blocks per SM of the persistent kernel of a kind and block size.
 int batch_blocks_per_sm(int precision, int kind, int threads);

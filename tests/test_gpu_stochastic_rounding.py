@@ -18,6 +18,7 @@ pytestmark = pytest.mark.gpu
 
 SCALE = {"f16": 10, "bf16": 6}
 W = np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4)
+W32 = W.astype(np.float32).astype(np.float64)   # the weights the device decodes against
 
 
 def _neighbours(x, precision):
@@ -62,7 +63,7 @@ def _uniform_bgk(lx, ly, precision, delta, rs, seed=1):
             lat.set_stochastic_rounding(True, seed)
         lat.set_geometry(1.0, tag, np.zeros(16 * nb), np.zeros(ly + 2, np.uint8))
         lat.set_populations(f, f)
-        d0 = _snap((lat.populations()[5, 5] - W) * 2.0 ** SCALE[precision], precision)
+        d0 = _snap((lat.populations()[5, 5] - W32) * 2.0 ** SCALE[precision], precision)
         lat.step(1)
         return lat.populations(), d0
 
@@ -77,16 +78,16 @@ def test_stochastic_rounding_is_unbiased(precision, delta):
     sum_d = float(np.sum(d0))
     tested = 0
     for group in ([0], [1, 2, 3, 4], [5, 6, 7, 8]):
-        e = W[group[0]] * sum_d                      # the stored value every node computes
+        e = W32[group[0]] * sum_d                    # the stored value every node computes
         lo, hi = _neighbours(e, precision)
         p = (e - lo) / (hi - lo)
-        d = (got[2:-2, 2:-2][..., group] - W[group]) * 2.0 ** s
+        d = (got[2:-2, 2:-2][..., group] - W32[group]) * 2.0 ** s
         up = np.abs(d - hi) < np.abs(d - lo)
         assert np.all(np.minimum(np.abs(d - hi), np.abs(d - lo)) < 0.25 * (hi - lo))
         n = up.size
         sigma = np.sqrt(max(p * (1 - p), 1e-4) / n)
         assert abs(up.mean() - p) < 5 * sigma, (precision, group, up.mean(), p)
-        dn = (nearest[2:-2, 2:-2][..., group] - W[group]) * 2.0 ** s
+        dn = (nearest[2:-2, 2:-2][..., group] - W32[group]) * 2.0 ** s
         rn = hi if abs(e - hi) < abs(e - lo) else lo
         assert np.all(np.abs(dn - rn) < 0.25 * (hi - lo))   # round to nearest: all the same
         tested += 0.05 < p < 0.95
@@ -187,23 +188,50 @@ def test_stochastic_rounding_arguments():
         with pytest.raises(lbgpu.LbError) as e:
             lat.set_stochastic_rounding(True, 1)
         assert e.value.code == 7
-    with lbgpu.Lattice(40, 20, "f16", "pull") as lat, lbgpu.Batch("f16") as batch:
+    with lbgpu.Lattice(40, 20, "f16", "pull") as lat:
         with pytest.raises(lbgpu.LbError) as e:
             lbgpu._check(lbgpu.lib().lbgpu_set_stochastic_rounding(lat.h, 2, 0))
         assert e.value.code == 3
-        lat.set_stochastic_rounding(True, 5)
-        lat.setup_cylinder(9, 11, 3, 0.02, 50.0, lbgpu.WALL_BOUNCEBACK, lbgpu.OUTLET_CONST)
-        with pytest.raises(lbgpu.LbError) as e:
-            batch.add(lat)
-        assert e.value.code == 7
-        lat.set_stochastic_rounding(False)
-        slot = batch.add(lat)
-        lat.set_stochastic_rounding(True, 5)      # switched on inside a batch: the batch refuses
-        with pytest.raises(lbgpu.LbError) as e:
-            batch.step(2)
-        assert e.value.code == 7
-        lat.set_stochastic_rounding(False)
-        batch.step(2)
-        batch.synchronize()
-        batch.remove(slot)
     lbgpu.clear_error()
+
+
+@pytest.mark.parametrize("precision", ["f16", "bf16"])
+@pytest.mark.parametrize("shape", [(32, 1), (128, 4)])
+def test_batch_members_round_like_the_lattice_alone(precision, shape):
+    """Members of every scheme, some rounding stochastically and some to nearest, one of them
+    switched on between calls: each ends bit-identical to its lattice stepped alone (57 steps:
+    the members' own first step, a replayed 50-step chunk and an odd remainder)."""
+    specs = [("pull", False, 7, True), ("aa", False, 8, True), ("pull", True, 9, True), ("pull", False, 0, False),
+             ("aa", True, 10, False)]
+
+    def make(scheme, shift, seed, rs):
+        return _channel(120 + 16 * seed, 37, precision, scheme, shift, seed=seed, rs=rs)
+
+    def alone(scheme, shift, seed, rs, late):
+        with make(scheme, shift, seed, rs and not late) as lat:
+            lat.step(20)
+            if late:
+                lat.set_stochastic_rounding(True, seed)
+            lat.step(37)
+            return lat.populations()
+
+    want = [alone(sc, sh, sd, rs, late=(i == 4)) for i, (sc, sh, sd, rs) in enumerate(specs)]
+    lats = [make(sc, sh, sd, rs) for sc, sh, sd, rs in specs]
+    try:
+        with lbgpu.Batch(precision) as batch:
+            for c in range(6):
+                batch.set_shape(c, *shape)
+            slots = [batch.add(lat) for lat in lats]
+            batch.step(20)
+            batch.synchronize()
+            lats[4].set_stochastic_rounding(True, 10)
+            batch.step(37)
+            batch.synchronize()
+            got = [lat.populations() for lat in lats]
+            for sl in slots:
+                batch.remove(sl)
+        for i, (g, w) in enumerate(zip(got, want)):
+            assert same(g, w), (i, specs[i], describe_diff(g, w))
+    finally:
+        for lat in lats:
+            lat.close()
