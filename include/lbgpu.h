@@ -286,6 +286,9 @@ int lbgpu_server_set_offset_scale(lbgpu_server *s, int scale_log2);
 /* FP16/BF16 servers: store each request's offsets from its inflow profile's equilibrium per
  * row (lbgpu_set_offset_shift) instead of from w_i. */
 int lbgpu_server_set_offset_shift(lbgpu_server *s, int on);
+/* FP16/BF16 servers: round each request's stored values stochastically
+ * (lbgpu_set_stochastic_rounding, seeded with the request id). */
+int lbgpu_server_set_stochastic_rounding(lbgpu_server *s, int on);
 int lbgpu_server_submit(lbgpu_server *s, const lbgpu_request *r, int *id);
 int lbgpu_server_run(lbgpu_server *s, int batched);
 int lbgpu_server_result(lbgpu_server *s, int id, lbgpu_result *out, double *ux, double *uy);

@@ -62,6 +62,7 @@ struct lbgpu_server {
     int check_every = 100;
     int scale_log2 = 10;
     bool shift = false;                      // 16-bit offsets from each request's inflow profile
+    bool rs = false;                         // 16-bit stochastic rounding, seeded by request id
     std::vector<Req> reqs;
     unsigned *d_change = nullptr;
     int cap_change = 0;
@@ -87,7 +88,7 @@ int scheme_of(const lbgpu_server *s, const lbgpu_request &r)
 }
 
 // Allocate and set up a request's lattice and its velocity snapshot.
-int start(lbgpu_server *s, Req &q)
+int start(lbgpu_server *s, Req &q, int id)
 {
     const lbgpu_request &r = q.spec;
     const int sch = scheme_of(s, r);
@@ -103,6 +104,8 @@ int start(lbgpu_server *s, Req &q)
             }
             if (int rc = lbgpu_set_offset_shift(q.lat, u.data())) return rc;
         }
+        if (s->rs)
+            if (int rc = lbgpu_set_stochastic_rounding(q.lat, 1, (unsigned)id)) return rc;
     }
     if (int rc = lbgpu_setup_cylinder(q.lat, r.obst_x, r.obst_y, r.obst_r, r.umax, r.re,
                                       LBGPU_WALL_BOUNCEBACK, LBGPU_OUTLET_CONST, nullptr))
@@ -233,6 +236,15 @@ int lbgpu_server_set_offset_shift(lbgpu_server *s, int on)
     return LB_OK;
 }
 
+int lbgpu_server_set_stochastic_rounding(lbgpu_server *s, int on)
+{
+    if (!s) return set_error(LB_ERR_ARG, "lbgpu_server_set_stochastic_rounding: null server");
+    if (on && s->precision != LBGPU_F16 && s->precision != LBGPU_BF16)
+        return set_error(LB_ERR_STATE, "lbgpu_server_set_stochastic_rounding: FP16/BF16 storage only");
+    s->rs = on != 0;
+    return LB_OK;
+}
+
 int lbgpu_server_set_offset_scale(lbgpu_server *s, int scale_log2)
 {
     if (!s || scale_log2 < -30 || scale_log2 > 30) return set_error(LB_ERR_ARG, "lbgpu_server_set_offset_scale");
@@ -289,7 +301,7 @@ int lbgpu_server_run(lbgpu_server *s, int batched)
             Req &q = s->reqs[order[qi]];
             const size_t need = request_bytes(s, q.spec, scheme_of(s, q.spec));
             if (used + need > s->budget || (!batched && !active.empty())) break;
-            if ((rc = start(s, q))) break;
+            if ((rc = start(s, q, order[qi]))) break;
             q.admit = now_s(t0);
             used += need;
             q.solo = batched && (long long)q.spec.lx * q.spec.ly >= s->solo_nodes && s->solo_nodes > 0;

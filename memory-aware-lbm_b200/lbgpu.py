@@ -132,6 +132,7 @@ def lib():
     L.lbgpu_server_set_threads.argtypes = [_vp, ctypes.c_int]
     L.lbgpu_server_set_solo_nodes.argtypes = [_vp, ctypes.c_longlong]
     L.lbgpu_server_set_offset_shift.argtypes = [_vp, ctypes.c_int]
+    L.lbgpu_server_set_stochastic_rounding.argtypes = [_vp, ctypes.c_int]
     L.lbgpu_server_set_offset_scale.argtypes = [_vp, ctypes.c_int]
     L.lbgpu_server_submit.argtypes = [_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int)]
     L.lbgpu_server_run.argtypes = [_vp, ctypes.c_int]
@@ -514,7 +515,7 @@ class Server:
     """lbgpu_server: continuous batching of cylinder-channel requests under an HBM budget."""
 
     def __init__(self, precision="f32", budget_bytes=8 << 30, check_every=100, scale=None,
-                 shift=False):
+                 shift=False, stochastic=False):
         self.precision = precision
         h = _vp()
         _check(lib().lbgpu_server_create(PRECISIONS[precision], int(budget_bytes),
@@ -526,6 +527,8 @@ class Server:
             _check(lib().lbgpu_server_set_offset_scale(h, default if scale is None else int(scale)))
             if shift:
                 _check(lib().lbgpu_server_set_offset_shift(h, 1))
+            if stochastic:
+                _check(lib().lbgpu_server_set_stochastic_rounding(h, 1))
 
     def close(self):
         if self.h:

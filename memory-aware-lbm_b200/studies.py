@@ -154,8 +154,9 @@ def serving_requests(n, seed=20260102, nmin=1e4, nmax=2e7, max_steps=5000, tol=1
     return out
 
 
-def _serve(prec, reqs, batched, budget, schemes=None, shapes=None, sample=(), shift=False):
-    with lbgpu.Server(prec, budget, 100, shift=shift and prec in lbgpu.DEFAULT_SCALE) as srv:
+def _serve(prec, reqs, batched, budget, schemes=None, shapes=None, sample=(), shift=False, rs=False):
+    half = prec in lbgpu.DEFAULT_SCALE
+    with lbgpu.Server(prec, budget, 100, shift=shift and half, stochastic=rs and half) as srv:
         for c, s in (schemes or {}).items():
             srv.set_scheme(c, s)
         for c, (w, npt) in (shapes or {}).items():
@@ -176,13 +177,15 @@ def _serve(prec, reqs, batched, budget, schemes=None, shapes=None, sample=(), sh
 
 
 def serving_study(precisions=("f32", "f16"), n=120, seed=20260102, budget_gb=150.0,
-                  load=0.95, sample_every=50, shift=0):
-    """shift=1: FP16/BF16 requests store offsets from their inflow profile (row shift)."""
+                  load=0.95, sample_every=50, shift=0, rs=0):
+    """shift=1: FP16/BF16 requests store offsets from their inflow profile (row shift); rs=1:
+    they round stochastically."""
     reqs = serving_requests(n, seed)
     work = [q["lx"] * q["ly"] * q["max_steps"] for q in reqs]
     budget = int(budget_gb * 1e9)
     sample = set(range(0, n, sample_every))
     out = {"requests": n, "seed": seed, "budget_gb": budget_gb, "offered_load": load, "row_shift": bool(shift),
+           "stochastic_rounding": bool(rs),
            "nodes_log_uniform": [1e4, 2e7], "max_steps": 5000, "tol": 1e-7,
            "fp64_sample": sorted(sample), "precisions": {}}
     rng = np.random.default_rng(seed + 1)
@@ -191,16 +194,16 @@ def serving_study(precisions=("f32", "f16"), n=120, seed=20260102, budget_gb=150
         schemes = {c: v["scheme"] for c, v in
                    tune_schemes(prec, [(q["lx"], q["ly"]) for q in reqs]).items()}
         # capacity: the batched rate on the whole request set at once (all arrive at t=0)
-        closed, _ = _serve(prec, reqs, True, budget, schemes, shift=shift)
+        closed, _ = _serve(prec, reqs, True, budget, schemes, shift=shift, rs=rs)
         cap = closed["mlups"] * 1e6
         mean_work = float(np.mean(work))
         rate = load * cap / mean_work            # requests per second
         t = np.cumsum(rng.exponential(1.0 / rate, n))
         stream = [dict(q, arrival=float(t[k] - t[0])) for k, q in enumerate(reqs)]
-        served, res = _serve(prec, stream, True, budget, schemes, sample=sample, shift=shift)
+        served, res = _serve(prec, stream, True, budget, schemes, sample=sample, shift=shift, rs=rs)
         # sequential plain solves: each request alone with the single-lattice pull kernel
-        seq, _ = _serve(prec, stream, False, budget, shift=shift)
-        seq_closed, _ = _serve(prec, reqs, False, budget, shift=shift)
+        seq, _ = _serve(prec, stream, False, budget, shift=shift, rs=rs)
+        seq_closed, _ = _serve(prec, reqs, False, budget, shift=shift, rs=rs)
         errs = []
         for k in sorted(sample):
             q = reqs[k]

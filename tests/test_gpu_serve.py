@@ -33,7 +33,8 @@ def requests(seed, n):
 
 
 def serve(precision, reqs, batched, budget, solo_nodes=None):
-    with lbgpu.Server(precision, budget, CHECK) as srv:
+    base, _, rs = lbgpu.storage_form(precision)
+    with lbgpu.Server(base, budget, CHECK, stochastic=rs) as srv:
         if solo_nodes is not None:
             srv.set_solo_nodes(solo_nodes)
         ids = [srv.submit(**q) for q in reqs]
@@ -42,10 +43,13 @@ def serve(precision, reqs, batched, budget, solo_nodes=None):
         return res, srv.stats()
 
 
-def alone(precision, q, steps):
-    with lbgpu.Lattice(q["lx"], q["ly"], precision, "pull") as lat:
-        if precision in lbgpu.DEFAULT_SCALE:
-            lat.set_offset_scale(lbgpu.DEFAULT_SCALE[precision])
+def alone(precision, q, steps, rid):
+    base, _, rs = lbgpu.storage_form(precision)
+    with lbgpu.Lattice(q["lx"], q["ly"], base, "pull") as lat:
+        if base in lbgpu.DEFAULT_SCALE:
+            lat.set_offset_scale(lbgpu.DEFAULT_SCALE[base])
+        if rs:   # the server seeds a request's rounding with its id
+            lat.set_stochastic_rounding(True, rid)
         lat.setup_cylinder(q["obst_x"], q["obst_y"], q["obst_r"], q["umax"], q["re"],
                            lbgpu.WALL_BOUNCEBACK, lbgpu.OUTLET_CONST)
         lat.step(steps)
@@ -54,11 +58,14 @@ def alone(precision, q, steps):
 
 
 @pytest.mark.parametrize("precision,solo_nodes", [("f32", 0), ("f16", 0), ("f64", 0),
-                                                 ("f32", 12000), ("f16", 12000)])
+                                                 ("f32", 12000), ("f16", 12000),
+                                                 ("f16r", 0), ("bf16r", 12000)])
 def test_served_results_match_sequential_and_alone(precision, solo_nodes):
-    """solo_nodes 0: every request a batch member; 12000: the larger ones step on their own."""
+    """solo_nodes 0: every request a batch member; 12000: the larger ones step on their own.
+    'r': stochastic rounding."""
     reqs = requests(7, 12)
-    budget = sum(lbgpu.lattice_bytes(q["lx"], q["ly"], precision) + 8 * q["lx"] * q["ly"]
+    base = lbgpu.storage_form(precision)[0]
+    budget = sum(lbgpu.lattice_bytes(q["lx"], q["ly"], base) + 8 * q["lx"] * q["ly"]
                  for q in reqs) // 3       # about a third of the requests fit at once
     mix, st_mix = serve(precision, reqs, True, budget, solo_nodes)
     solo = [r["solo"] for r in mix]
@@ -76,7 +83,7 @@ def test_served_results_match_sequential_and_alone(precision, solo_nodes):
         assert a["admit"] >= q["arrival"] and a["finish"] > a["admit"], k
         assert np.array_equal(a["ux"], b["ux"]) and np.array_equal(a["uy"], b["uy"]), k
         assert a["last_change"] == b["last_change"], k
-        ux, uy = alone(precision, q, a["steps"])
+        ux, uy = alone(precision, q, a["steps"], k)
         assert np.array_equal(a["ux"], ux) and np.array_equal(a["uy"], uy), k
         if q["tol"] == 1.0:        # any change after the first interval is below 1
             assert a["converged"] == 1 and a["steps"] == CHECK, k
@@ -101,9 +108,9 @@ def test_server_schemes_and_late_arrivals():
         ids = [srv.submit(**q) for q in reqs]
         srv.run(True)
         res = [srv.result(i, fields=True) for i in ids]
-    for q, r in zip(reqs, res):
+    for k, (q, r) in enumerate(zip(reqs, res)):
         assert r["steps"] == q["max_steps"] and r["admit"] >= q["arrival"]
-        ux, uy = alone("f32", q, r["steps"])
+        ux, uy = alone("f32", q, r["steps"], k)
         assert np.array_equal(r["ux"], ux) and np.array_equal(r["uy"], uy)
 
 
