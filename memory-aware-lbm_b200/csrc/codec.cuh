@@ -69,10 +69,14 @@ template <> struct Codec<__nv_bfloat16> {
 //
 // The random bits of a value depend only on (seed, collision number k, node, direction), so every
 // scheme that produces the same post-collision value stores the same bits:
-//   key_k = rs_key(seed, k)                      per collision (host), never 0
-//   h     = rs_mix((Y (lx + 2) + X) ^ key_k)     per node
-//   r_i   = bits 16..31 of h * K_i               per direction, K_i odd
-// rs_mix is the 32-bit integer hash "lowbias32" (C. Wellons, hash-prospector).
+//   key_k = rs_key(seed, k)                              per collision (host), never 0
+//   H     = rs_mix((Y (lx + 2) + x0) ^ key_k)            per quad of nodes x0..x0+3 of a row,
+//                                                        x0 = X - ((X - 1) mod 4)
+//   h     = H * C_q,  q = X - x0                         per node, C_q odd
+//   r_i   = bits 16..31 of h * K_i                       per direction, K_i odd
+// One hash serves four nodes (the 16-bit kernels' unit of work); the two multiplies fold into
+// one by a constant there.  rs_mix is the 32-bit integer hash "lowbias32" (C. Wellons,
+// hash-prospector).
 __host__ __device__ __forceinline__ unsigned rs_mix(unsigned x)
 {
     x ^= x >> 16;
@@ -87,6 +91,11 @@ __host__ __device__ __forceinline__ unsigned rs_key(unsigned seed, unsigned long
 {
     const unsigned lo = (unsigned)k, hi = (unsigned)(k >> 32);
     return rs_mix(seed ^ rs_mix(lo ^ rs_mix(hi + 0x9e3779b9u))) | 1u;
+}
+
+__host__ __device__ __forceinline__ unsigned rs_place(unsigned hq, int q)
+{
+    return hq * (0x85ebca6bu + (unsigned)q * 0x3c6ef372u);   // odd for every q
 }
 
 __host__ __device__ __forceinline__ unsigned rs_dir(unsigned h, int i)

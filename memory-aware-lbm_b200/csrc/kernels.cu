@@ -206,7 +206,10 @@ template <> struct Work<__nv_bfloat16> {
 template <class S, bool RS>
 __device__ __forceinline__ unsigned rs_node(const Geo &g, unsigned key, int X, int Y)
 {
-    if constexpr (RS && sizeof(S) == 2) return rs_mix(((unsigned)Y * (unsigned)(g.lx + 2) + (unsigned)X) ^ key);
+    if constexpr (RS && sizeof(S) == 2) {
+        const int q = (X - 1) & 3;
+        return rs_place(rs_mix(((unsigned)Y * (unsigned)(g.lx + 2) + (unsigned)(X - q)) ^ key), q);
+    }
     return 0u;
 }
 
@@ -441,9 +444,9 @@ __device__ __forceinline__ void pull_node(const Geo &g, const S *__restrict__ sr
 template <class S, bool RS>
 __device__ __forceinline__ void quad_words(const Geo &g, unsigned key, int x0, int Y, unsigned h[4])
 {
-    const unsigned id = (unsigned)Y * (unsigned)(g.lx + 2) + (unsigned)x0;
+    const unsigned hq = RS ? rs_mix(((unsigned)Y * (unsigned)(g.lx + 2) + (unsigned)x0) ^ key) : 0u;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) h[k] = RS ? rs_mix((id + (unsigned)k) ^ key) : 0u;
+    for (int k = 0; k < 4; ++k) h[k] = rs_place(hq, k);
 }
 
 // Direction i of a quad's four working values as the stored aligned word pair.
