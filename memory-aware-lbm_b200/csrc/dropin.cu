@@ -53,8 +53,8 @@ struct DropIn {
     bool bc_force = true;       // upload tables at the next refresh even if unchanged
     bool tmp_is_stream = false; // tmpLattice holds the stream of lattice (collide_with_stream)
     int sync_mode = LB_SYNC_OUTLET;
-    bool pinned[2] = {false, false};
-    void *pinned_ptr[2] = {nullptr, nullptr};
+    bool pinned[3] = {false, false, false};         // host arrays, then the dynamics pointers
+    void *pinned_ptr[3] = {nullptr, nullptr, nullptr};
     std::vector<uint64_t> dynp;          // host Dynamics* of every node, [X*(ly+2)+Y]
     uint64_t *dynp_dev = nullptr;
     std::vector<const void *> slot_src;  // [8*nb] boundary data object of each table slot
@@ -228,11 +228,13 @@ void pin_host(Simulation *sim, DropIn *c)
 {
     const char *e = getenv("LBGPU_PIN");
     if (e && e[0] == '0') return;
-    const size_t bytes = (size_t)(sim->lx + 2) * (sim->ly + 2) * sizeof(Node);
-    Node *chunks[2] = {sim->memoryChunk, sim->tmpMemoryChunk};
-    for (int k = 0; k < 2; ++k) {
-        if (c->pinned[k] || !chunks[k]) continue;
-        if (cudaHostRegister(chunks[k], bytes, cudaHostRegisterPortable) == cudaSuccess) {
+    const size_t nodes = (size_t)(sim->lx + 2) * (sim->ly + 2);
+    // the dynamics pointers too: the first read-out uploads them (the vector never reallocates)
+    void *chunks[3] = {sim->memoryChunk, sim->tmpMemoryChunk, c->dynp.data()};
+    const size_t bytes[3] = {nodes * sizeof(Node), nodes * sizeof(Node), c->dynp.size() * sizeof(uint64_t)};
+    for (int k = 0; k < 3; ++k) {
+        if (c->pinned[k] || !chunks[k] || !bytes[k]) continue;
+        if (cudaHostRegister(chunks[k], bytes[k], cudaHostRegisterPortable) == cudaSuccess) {
             c->pinned[k] = true;
             c->pinned_ptr[k] = chunks[k];
         } else {
@@ -446,7 +448,7 @@ void destructSim(Simulation *sim)
             if (c->dynp_dev) cudaFree(c->dynp_dev);
             c->L.destroy();
         }
-        for (int k = 0; k < 2; ++k)
+        for (int k = 0; k < 3; ++k)   // before the dynamics-pointer vector goes with c
             if (c->pinned[k]) cudaHostUnregister(c->pinned_ptr[k]);
         delete c;
     }
