@@ -590,7 +590,7 @@ __global__ void __launch_bounds__(BX) k_stream(Geo g, const S *__restrict__ src,
 // on row YL - 2, which it writes.  Halo work is two columns a side and two rows a segment end
 // (a few percent), and the shared memory a block needs is small enough for several blocks a SM.
 template <class S, int W>
-constexpr size_t sweep2_r0_bytes() { return (3 * 9 * (size_t)(W + 4) * sizeof(S) + 15) / 16 * 16; }
+constexpr size_t sweep2_r0_bytes() { return (4 * 9 * (size_t)(W + 4) * sizeof(S) + 15) / 16 * 16; }
 template <class S, int W>
 constexpr size_t sweep2_smem_bytes() { return sweep2_r0_bytes<S, W>() + 3 * 9 * (size_t)(W + 2) * sizeof(S); }
 
@@ -603,26 +603,44 @@ __global__ void __launch_bounds__(W) k_sweep2(Geo g, const S *__restrict__ src, 
 {
     constexpr int W0 = W + 4, W1 = W + 2;
     extern __shared__ __align__(16) unsigned char sweep_smem[];
-    auto r0 = reinterpret_cast<S (*)[9][W0]>(sweep_smem);                 // C_n rows [3], slot = row mod 3
+    auto r0 = reinterpret_cast<S (*)[9][W0]>(sweep_smem);                 // C_n rows [4], slot = row mod 4
     auto r1 = reinterpret_cast<S (*)[9][W1]>(sweep_smem + sweep2_r0_bytes<S, W>());   // C_{n+1} rows [3]
     const int x0 = 1 + blockIdx.x * W, y0 = 1 + blockIdx.y * H;
     const int tx = threadIdx.x;
     const int yend = min(y0 + H, g.ly + 1);           // rows y0 .. yend-1 are this block's
-    for (int t = 0; y0 - 2 + t - 2 < yend; ++t) {
-        const int YL = y0 - 2 + t;
-        // C_n row YL (positions outside the array are never read)
+    // C_n row YL into ring slot YL mod 4 by asynchronous copies (cp.async; one commit group a row,
+    // empty for rows outside the array).  A copy unit is one element of 4 or 8 bytes, or two
+    // 2-byte elements from an even k (element x0-2+k of the row sits at an even index then, so
+    // the pair is 4-byte aligned); units may cover the row's padding (X = -1 or lx + 2), which is
+    // inside the allocation and never read back.
+    constexpr int E = sizeof(S) >= 4 ? 1 : 2;
+    constexpr unsigned UB = E * sizeof(S);
+    auto fetch = [&](int YL) {
         if (YL >= 0 && YL <= g.ly + 1) {
-            const int sl = (YL + 3) % 3;
-            for (int k = tx; k < W0; k += W) {
-                const int X = x0 - 2 + k;
-                if (X >= 0 && X <= g.lx + 1) {
+            const int sl = (YL + 4) % 4;
+            for (int u = tx; u < W0 / E; u += W) {
+                const int k = u * E, X = x0 - 2 + k;
+                if (X + E - 1 >= 0 && X <= g.lx + 1) {
                     const long long o = g.idx(X, YL);
 #pragma unroll
-                    for (int i = 0; i < 9; ++i) r0[sl][i][k] = plane(src, g, i)[o];
+                    for (int i = 0; i < 9; ++i) {
+                        const unsigned d = (unsigned)__cvta_generic_to_shared(&r0[sl][i][k]);
+                        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(plane(src, g, i) + o),
+                                     "n"(UB) : "memory");
+                    }
                 }
             }
         }
-        __syncthreads();
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    fetch(y0 - 2);
+    for (int t = 0; y0 - 2 + t - 2 < yend; ++t) {
+        const int YL = y0 - 2 + t;
+        // row YL + 1 flies while rows YL - 1 and YL - 2 are computed; its slot held row YL - 3,
+        // last read before the previous iteration's second barrier
+        fetch(YL + 1);
+        asm volatile("cp.async.wait_group 1;" ::: "memory");   // this thread's copies of row YL landed
+        __syncthreads();                                      // everyone's
         // step n+1 on row YL - 1, columns x0-1 .. x0+W
         const int Y1 = YL - 1;
         if (Y1 >= y0 - 1 && Y1 >= 1 && Y1 <= g.ly && Y1 <= yend) {
@@ -635,7 +653,7 @@ __global__ void __launch_bounds__(W) k_sweep2(Geo g, const S *__restrict__ src, 
 #pragma unroll
                 for (int i = 0; i < 9; ++i) {
                     const int sx = X - cx(i), sy = Y1 - cy(i);
-                    f[i] = Work<S>::load(g.interior(sx, sy) ? r0[(sy + 3) % 3][i][sx - x0 + 2]
+                    f[i] = Work<S>::load(g.interior(sx, sy) ? r0[(sy + 4) % 4][i][sx - x0 + 2]
                                                             : side_a[(size_t)i * g.nper + p], i, inv);
                 }
                 collide_w<S>(bc, g, tag[g.idx(X, Y1)], X, Y1, f, omega, sc, inv);
@@ -677,6 +695,7 @@ __global__ void __launch_bounds__(W) k_sweep2(Geo g, const S *__restrict__ src, 
             }
         }
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");   // the last prefetch lands before the block ends
 }
 
 // After k_sweep2: the scratch stale slots into parity (n+1)&1, and the ghost rings of the two
