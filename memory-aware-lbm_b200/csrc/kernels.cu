@@ -584,18 +584,20 @@ __global__ void __launch_bounds__(BX) k_stream(Geo g, const S *__restrict__ src,
 // in the buffer two single steps would not have left it in, and the read-outs take ghost values
 // from the other buffer.
 //
-// The kernel is a sweep (the shape of the reference's tight variants): a block of W threads owns a strip of W columns and a segment of H rows and walks down it,
-// keeping three rows of C_n (W + 4 wide) and three rows of C_{n+1} (W + 2 wide) in shared
-// memory.  Iteration t loads C_n row YL = y0 - 2 + t, computes C_{n+1} on row YL - 1 and C_{n+2}
-// on row YL - 2, which it writes.  Halo work is two columns a side and two rows a segment end
-// (a few percent), and the shared memory a block needs is small enough for several blocks a SM.
+// The kernel is a sweep (the shape of the reference's tight variants): a block of W + 2 threads
+// owns a strip of W columns and a segment of H rows and walks down it, keeping four rows of C_n
+// (W + 4 wide) and three rows of C_{n+1} (W + 2 wide) in shared memory.  Iteration t has C_n row
+// YL = y0 - 2 + t (fetched asynchronously during the previous iteration), fetches row YL + 1,
+// computes C_{n+1} on row YL - 1 (W + 2 nodes: one a thread) and C_{n+2} on row YL - 2, which it
+// writes.  Halo work is two columns a side and two rows a segment end (a few percent), and the
+// shared memory a block needs is small enough for several blocks a SM.
 template <class S, int W>
 constexpr size_t sweep2_r0_bytes() { return (4 * 9 * (size_t)(W + 4) * sizeof(S) + 15) / 16 * 16; }
 template <class S, int W>
 constexpr size_t sweep2_smem_bytes() { return sweep2_r0_bytes<S, W>() + 3 * 9 * (size_t)(W + 2) * sizeof(S); }
 
 template <class S, int W, int H, bool RS>
-__global__ void __launch_bounds__(W) k_sweep2(Geo g, const S *__restrict__ src, S *__restrict__ dst,
+__global__ void __launch_bounds__(W + 2) k_sweep2(Geo g, const S *__restrict__ src, S *__restrict__ dst,
                                              const uint8_t *__restrict__ tag, const double *__restrict__ bc,
                                              double omega, const S *__restrict__ side_a,
                                              S *__restrict__ side_tmp, S *__restrict__ side_b, float sc,
@@ -618,7 +620,7 @@ __global__ void __launch_bounds__(W) k_sweep2(Geo g, const S *__restrict__ src, 
     auto fetch = [&](int YL) {
         if (YL >= 0 && YL <= g.ly + 1) {
             const int sl = (YL + 4) % 4;
-            for (int u = tx; u < W0 / E; u += W) {
+            for (int u = tx; u < W0 / E; u += W + 2) {
                 const int k = u * E, X = x0 - 2 + k;
                 if (X + E - 1 >= 0 && X <= g.lx + 1) {
                     const long long o = g.idx(X, YL);
@@ -644,7 +646,7 @@ __global__ void __launch_bounds__(W) k_sweep2(Geo g, const S *__restrict__ src, 
         // step n+1 on row YL - 1, columns x0-1 .. x0+W
         const int Y1 = YL - 1;
         if (Y1 >= y0 - 1 && Y1 >= 1 && Y1 <= g.ly && Y1 <= yend) {
-            for (int k = tx; k < W1; k += W) {
+            for (int k = tx; k < W1; k += W + 2) {
                 const int X = x0 - 1 + k;
                 if (X < 1 || X > g.lx) continue;
                 const bool edge = g.perimeter(X, Y1);
@@ -673,7 +675,7 @@ __global__ void __launch_bounds__(W) k_sweep2(Geo g, const S *__restrict__ src, 
         // step n+2 on row YL - 2, columns x0 .. x0+W-1, to the other buffer
         const int Y2 = YL - 2;
         const int X = x0 + tx;
-        if (Y2 >= y0 && Y2 < yend && X <= g.lx) {
+        if (tx < W && Y2 >= y0 && Y2 < yend && X <= g.lx) {
             const bool edge = g.perimeter(X, Y2);
             const int p = edge ? g.pidx(X, Y2) : 0;
             typename Work<S>::W f[9];
@@ -1491,7 +1493,7 @@ static void launch_sweep2_t(const DevLattice &d, int src, int n_par, cudaStream_
     constexpr size_t smem = sweep2_smem_bytes<S, W>();
     cudaFuncSetAttribute(k_sweep2<S, W, H, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid(cdiv(d.g.lx, W), cdiv(d.g.ly, H));
-    k_sweep2<S, W, H, RS><<<grid, W, smem, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
+    k_sweep2<S, W, H, RS><<<grid, W + 2, smem, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
                                          SIDE<S>(d, n_par + 1), SIDE_TMP<S>(d), SIDE<S>(d, n_par), d.scale,
                                          d.inv_scale);
 }
@@ -1499,15 +1501,15 @@ static void launch_sweep2_t(const DevLattice &d, int src, int n_par, cudaStream_
 void launch_pull2(const DevLattice &d, int src, int n_par, cudaStream_t s)
 {
     switch (d.precision) {
-    case LBGPU_F64: launch_sweep2_t<double, 128, 128>(d, src, n_par, s); break;
-    case LBGPU_F32: launch_sweep2_t<float, 128, 128>(d, src, n_par, s); break;
+    case LBGPU_F64: launch_sweep2_t<double, 126, 128>(d, src, n_par, s); break;
+    case LBGPU_F32: launch_sweep2_t<float, 126, 128>(d, src, n_par, s); break;
     case LBGPU_F16:
-        if (d.g.rs_key) launch_sweep2_t<__half, 128, 128, true>(d, src, n_par, s);
-        else launch_sweep2_t<__half, 128, 128>(d, src, n_par, s);
+        if (d.g.rs_key) launch_sweep2_t<__half, 126, 128, true>(d, src, n_par, s);
+        else launch_sweep2_t<__half, 126, 128>(d, src, n_par, s);
         break;
     default:
-        if (d.g.rs_key) launch_sweep2_t<__nv_bfloat16, 128, 128, true>(d, src, n_par, s);
-        else launch_sweep2_t<__nv_bfloat16, 128, 128>(d, src, n_par, s);
+        if (d.g.rs_key) launch_sweep2_t<__nv_bfloat16, 126, 128, true>(d, src, n_par, s);
+        else launch_sweep2_t<__nv_bfloat16, 126, 128>(d, src, n_par, s);
         break;
     }
     const int nthreads = std::max(d.g.nper, d.g.nghost());
