@@ -191,3 +191,21 @@ def test_reference_keeps_its_own_symbols_when_the_gpu_library_is_global():
         "out = O.run_reference(O.Cylinder.reference_driver(64, 48), 'tight', 200)\n"
         "sys.exit(0 if check_golden(g['ref_driver_64x48_200'], out) else 1)\n")
     assert subprocess.run([sys.executable, "-c", code]).returncode == 0
+
+
+def test_storage_names():
+    """bench.py and the studies name storage forms; 's' and 'r' are 16-bit options only."""
+    assert lbgpu.storage_form("f64") == ("f64", False, False)
+    assert lbgpu.storage_form("f16s") == ("f16", True, False)
+    assert lbgpu.storage_form("bf16r") == ("bf16", False, True)
+    assert lbgpu.storage_form("f16sr") == ("f16", True, True)
+    for bad in ("f32r", "f64s", "f16rs", "fp16", ""):
+        with pytest.raises(ValueError):
+            lbgpu.storage_form(bad)
+
+
+def test_stochastic_rounding_setter_rejects_a_null_lattice():
+    """The setter validates its handle before touching a device (no GPU here)."""
+    rc = lbgpu.lib().lbgpu_set_stochastic_rounding(None, 1, 0)
+    assert rc != 0
+    lbgpu.clear_error()
