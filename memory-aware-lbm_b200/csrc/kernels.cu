@@ -314,6 +314,44 @@ __device__ __forceinline__ void collide_w(const double *__restrict__ bc, const G
     }
 }
 
+// L2 prefetch for the block a few rows further down the grid (blocks run roughly in row order,
+// so those rows are read soon after, from L2): one thread a block issues the nine row segments
+// that block reads, nodes x0 .. x0 + NW - 1 of rows Y - c_iy widened by 16 bytes a side
+// (cp.async.bulk.prefetch.L2: no completion to wait for).  A segment starts on a 16-byte boundary
+// (the layout puts X = 1 on a 128-byte line and x0 - 1 is a multiple of NW) and is a multiple of
+// 16 bytes long; blocks whose segment would pass the row's pitch skip it, as do rows past ly, so
+// every prefetched byte is inside its plane.
+// Distances measured on the 16384x4096 channel (GLUPS without -> with): 16-bit pull 16 rows
+// (157.7 -> 170.9 FP16, 157.7 -> 171.7 BF16); FP32 pull 8 rows (88.0 -> 90.3); FP64 pull none (it
+// runs at the copy bandwidth already, and 8 / 16 / 32 rows cost 1 / 10 / 29 %: rows fetched that
+// early are evicted before they are read).
+#ifndef LBGPU_PF_ROWS
+#define LBGPU_PF_ROWS 16       // 16-bit pull kernel
+#endif
+#ifndef LBGPU_PF_ROWS_F32
+#define LBGPU_PF_ROWS_F32 8    // FP32 pull kernel
+#endif
+#ifndef LBGPU_PF_ROWS_AA
+#define LBGPU_PF_ROWS_AA 16    // 16-bit AA kernels (140.4 -> 150.8 FP16)
+#endif
+template <class S>
+constexpr int pf_rows_wide() { return sizeof(S) == 4 ? LBGPU_PF_ROWS_F32 : 0; }
+// ROWS: which row of plane i a node of row Y reads: 0 row Y - c_iy (pull), 1 row Y (AA even
+// step), 2 row Y + c_iy (AA odd step, whose direction i comes from plane opp(i) at row Y - c_iy).
+template <class S, int NW, int ROWS = 0>
+__device__ __forceinline__ void prefetch_rows_l2(const Geo &g, const S *__restrict__ src, int x0, int Y)
+{
+    constexpr int H = 16 / (int)sizeof(S);                          // halo elements a side
+    constexpr unsigned BYTES = (unsigned)((NW + 2 * H) * sizeof(S));
+    if (Y > g.ly || (long long)(x0 + NW + H - 1) + g.xoff - 1 >= g.pitch) return;
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                     ::"l"(plane(src, g, i) + g.idx(x0 - H, ROWS == 0 ? Y - cy(i) : (ROWS == 1 ? Y : Y + cy(i)))),
+                     "n"(BYTES)
+                     : "memory");
+}
+
 // ---- pull scheme --------------------------------------------------------------------------
 
 // In-place collision of every interior node (form L -> form C); the perimeter nodes also
@@ -373,6 +411,8 @@ __global__ void __launch_bounds__(BX) k_pull(Geo g, const S *__restrict__ src, S
     using R = typename C::R;
     const int X = blockIdx.x * BX + threadIdx.x + 1;
     const int Y = blockIdx.y + (GHOSTS ? 0 : 1);
+    if (!GHOSTS && pf_rows_wide<S>() > 0 && threadIdx.x == 0)
+        prefetch_rows_l2<S, BX>(g, src, 1 + BX * (int)blockIdx.x, Y + pf_rows_wide<S>());
     if (X > g.lx + (GHOSTS ? 1 : 0)) return;
     const long long o = g.idx(X, Y);
     if (GHOSTS && !g.interior(X, Y)) {
@@ -546,6 +586,8 @@ __global__ void __launch_bounds__(BX, SHIFT ? 7 : 8) k_pull4h(Geo g, const S *__
                                                const double *__restrict__ bc, double omega,
                                                S *__restrict__ side, float sc, float inv)
 {
+    if (LBGPU_PF_ROWS > 0 && threadIdx.x == 0)
+        prefetch_rows_l2<S, 4 * BX>(g, src, 1 + 4 * BX * (int)blockIdx.x, (int)blockIdx.y + 1 + LBGPU_PF_ROWS);
     const int t = blockIdx.x * BX + threadIdx.x;
     pull_quad<S, SHIFT, RS>(g, src, dst, tag, bc, omega, side, sc, inv, 1 + 4 * t, blockIdx.y + 1, threadIdx.x & 31,
                             g.rs_key);
@@ -869,6 +911,8 @@ __global__ void __launch_bounds__(BX, SHIFT ? 7 : 8) k_aa4_even(Geo g, S *__rest
 {
     using H = Half2Ops<S>;
     const int x0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x), Y = blockIdx.y + 1, lane = threadIdx.x & 31;
+    if (LBGPU_PF_ROWS_AA > 0 && threadIdx.x == 0)
+        prefetch_rows_l2<S, 4 * BX, 1>(g, a, 1 + 4 * BX * (int)blockIdx.x, Y + LBGPU_PF_ROWS_AA);
     const unsigned key = g.rs_key;
     if (!aa_quad_vec<S, SHIFT>(g, x0, Y, lane)) {
         for (int k = 0; k < 4; ++k)
@@ -897,6 +941,8 @@ __global__ void __launch_bounds__(BX, SHIFT ? 6 : 7) k_aa4_odd(Geo g, S *__restr
 {
     using H = Half2Ops<S>;
     const int x0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x), Y = blockIdx.y + 1, lane = threadIdx.x & 31;
+    if (LBGPU_PF_ROWS_AA > 0 && threadIdx.x == 0)
+        prefetch_rows_l2<S, 4 * BX, 2>(g, a, 1 + 4 * BX * (int)blockIdx.x, Y + LBGPU_PF_ROWS_AA);
     const unsigned key = g.rs_key;
     if (!aa_quad_vec<S, SHIFT>(g, x0, Y, lane)) {
         for (int k = 0; k < 4; ++k)
