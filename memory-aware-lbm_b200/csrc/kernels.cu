@@ -1034,6 +1034,12 @@ __global__ void __launch_bounds__(BX, SHIFT ? 6 : 7) k_aa4_odd(Geo g, S *__restr
 // at 40 registers against 86 % for the single-lattice pull kernel at 32), so the minimum blocks
 // per SM below cap the registers as far as that costs no (or a few bytes of) spills: 2048
 // threads a SM leave 32 registers a thread, 1280 leave 48, 1024 leave 64, 768 leave 80.
+// The 16-bit quad list: 8 blocks of 128 threads (64 registers, with spills) measured 96.8 GLUPS
+// on the 512-channel batch against 95.5 at 6 blocks (80 registers), 88.5 at 5 and 79.4 at 4
+// (127 registers, no spills): occupancy beats the spills here.
+#ifndef LBGPU_PULL4_MINB
+#define LBGPU_PULL4_MINB 8
+#endif
 template <class S, int KIND, bool PERSIST, int BT>
 constexpr int batch_min_blocks()
 {
@@ -1041,7 +1047,7 @@ constexpr int batch_min_blocks()
     if (sizeof(S) == 8) b128 = KIND == BATCH_PULL ? (PERSIST ? 6 : 10) : (KIND == BATCH_AA_EVEN ? 6 : 5);
     else if (KIND == BATCH_PULL) b128 = PERSIST ? 8 : 16;
     else if (KIND == BATCH_AA_EVEN) b128 = PERSIST ? 8 : 10;
-    else if (KIND == BATCH_PULL4) b128 = 6;
+    else if (KIND == BATCH_PULL4) b128 = LBGPU_PULL4_MINB;
     else b128 = (sizeof(S) == 4 && !PERSIST) ? 6 : 8;
     return b128 * 128 / BT > 0 ? b128 * 128 / BT : 1;
 }
