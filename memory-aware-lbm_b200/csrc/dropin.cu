@@ -269,10 +269,8 @@ DropIn *prepare(Simulation *sim, const char *fn, bool tables = true)
     }
     Lattice &L = c->L;
     if (!c->created && create_device(sim, c) != LB_OK) return nullptr;
-    if (c->tags_dirty) {
-        if (scan_dynamics(sim, c) != LB_OK) return nullptr;
-        c->tags_dirty = false;
-    }
+    // The population uploads go first: they are asynchronous copies from the pinned host
+    // arrays, so the host's scan of the dynamics pointers below runs while they transfer.
     if (!c->uploaded) {
         L.launches = 0;
         if (L.upload_records(0, reinterpret_cast<const double *>(chunk_of(sim->lattice)), 10, 0, sim->lx + 2) ||
@@ -292,6 +290,10 @@ DropIn *prepare(Simulation *sim, const char *fn, bool tables = true)
             if (L.upload_records(L.cur, src, 10, 0, sim->lx + 2)) return nullptr;
         }
         c->pops_dirty = false;
+    }
+    if (c->tags_dirty) {
+        if (scan_dynamics(sim, c) != LB_OK) return nullptr;
+        c->tags_dirty = false;
     }
     if (tables && refresh_params(c) != LB_OK) return nullptr;
     return c;
