@@ -328,6 +328,9 @@ __device__ __forceinline__ void collide_w(const double *__restrict__ bc, const G
 #ifndef LBGPU_PF_ROWS
 #define LBGPU_PF_ROWS 16       // 16-bit pull kernel
 #endif
+#ifndef LBGPU_PF_TAGS
+#define LBGPU_PF_TAGS 1        // the 16-bit pull kernel's tag row as well (167.4 -> 169.5 FP16)
+#endif
 #ifndef LBGPU_PF_ROWS_F32
 #define LBGPU_PF_ROWS_F32 8    // FP32 pull kernel
 #endif
@@ -594,8 +597,15 @@ __global__ void __launch_bounds__(BX, SHIFT ? 7 : 8) k_pull4h(Geo g, const S *__
                                                const double *__restrict__ bc, double omega,
                                                S *__restrict__ side, float sc, float inv)
 {
-    if (LBGPU_PF_ROWS > 0 && threadIdx.x == 0)
+    if (LBGPU_PF_ROWS > 0 && threadIdx.x == 0) {
         prefetch_rows_l2<S, 4 * BX>(g, src, 1 + 4 * BX * (int)blockIdx.x, (int)blockIdx.y + 1 + LBGPU_PF_ROWS);
+#if LBGPU_PF_TAGS
+        // the same block's tag row: one byte a node, x0 - 1 a multiple of 512 (16-byte aligned)
+        const int yt = (int)blockIdx.y + 1 + LBGPU_PF_ROWS, xt = 1 + 4 * BX * (int)blockIdx.x;
+        if (yt <= g.ly && (long long)(xt + 4 * BX - 1) + g.xoff - 1 < g.pitch)
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(tag + g.idx(xt, yt)), "n"(4 * BX) : "memory");
+#endif
+    }
     const int t = blockIdx.x * BX + threadIdx.x;
     pull_quad<S, SHIFT, RS>(g, src, dst, tag, bc, omega, side, sc, inv, 1 + 4 * t, blockIdx.y + 1, threadIdx.x & 31,
                             g.rs_key);
