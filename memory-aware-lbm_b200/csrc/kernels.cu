@@ -331,6 +331,9 @@ __device__ __forceinline__ void collide_w(const double *__restrict__ bc, const G
 #ifndef LBGPU_PF_TAGS
 #define LBGPU_PF_TAGS 1        // the 16-bit pull kernel's tag row as well (167.4 -> 169.5 FP16)
 #endif
+// The tag row is prefetched with the population rows by the AA kernels too (about 2 % each:
+// FP16 149.3 -> 152.1, FP32 83.7 -> 85.4, FP64 44.5 -> 45.4), not by the FP32 pull kernel
+// (no change there).
 #ifndef LBGPU_PF_ROWS_F32
 #define LBGPU_PF_ROWS_F32 8    // FP32 pull kernel
 #endif
@@ -350,11 +353,14 @@ constexpr int pf_rows_aa_wide() { return sizeof(S) == 4 ? LBGPU_PF_ROWS_AA_F32 :
 // ROWS: which row of plane i a node of row Y reads: 0 row Y - c_iy (pull), 1 row Y (AA even
 // step), 2 row Y + c_iy (AA odd step, whose direction i comes from plane opp(i) at row Y - c_iy).
 template <class S, int NW, int ROWS = 0>
-__device__ __forceinline__ void prefetch_rows_l2(const Geo &g, const S *__restrict__ src, int x0, int Y)
+__device__ __forceinline__ void prefetch_rows_l2(const Geo &g, const S *__restrict__ src, int x0, int Y,
+                                                 const uint8_t *__restrict__ tag = nullptr)
 {
     constexpr int H = 16 / (int)sizeof(S);                          // halo elements a side
     constexpr unsigned BYTES = (unsigned)((NW + 2 * H) * sizeof(S));
     if (Y > g.ly || (long long)(x0 + NW + H - 1) + g.xoff - 1 >= g.pitch) return;
+    if (tag)   // the block's tag row: one byte a node, 16-byte aligned like the rows
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(tag + g.idx(x0, Y)), "n"(NW) : "memory");
 #pragma unroll
     for (int i = 0; i < 9; ++i)
         asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
@@ -597,15 +603,9 @@ __global__ void __launch_bounds__(BX, SHIFT ? 7 : 8) k_pull4h(Geo g, const S *__
                                                const double *__restrict__ bc, double omega,
                                                S *__restrict__ side, float sc, float inv)
 {
-    if (LBGPU_PF_ROWS > 0 && threadIdx.x == 0) {
-        prefetch_rows_l2<S, 4 * BX>(g, src, 1 + 4 * BX * (int)blockIdx.x, (int)blockIdx.y + 1 + LBGPU_PF_ROWS);
-#if LBGPU_PF_TAGS
-        // the same block's tag row: one byte a node, x0 - 1 a multiple of 512 (16-byte aligned)
-        const int yt = (int)blockIdx.y + 1 + LBGPU_PF_ROWS, xt = 1 + 4 * BX * (int)blockIdx.x;
-        if (yt <= g.ly && (long long)(xt + 4 * BX - 1) + g.xoff - 1 < g.pitch)
-            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(tag + g.idx(xt, yt)), "n"(4 * BX) : "memory");
-#endif
-    }
+    if (LBGPU_PF_ROWS > 0 && threadIdx.x == 0)
+        prefetch_rows_l2<S, 4 * BX>(g, src, 1 + 4 * BX * (int)blockIdx.x, (int)blockIdx.y + 1 + LBGPU_PF_ROWS,
+                                    LBGPU_PF_TAGS ? tag : nullptr);
     const int t = blockIdx.x * BX + threadIdx.x;
     pull_quad<S, SHIFT, RS>(g, src, dst, tag, bc, omega, side, sc, inv, 1 + 4 * t, blockIdx.y + 1, threadIdx.x & 31,
                             g.rs_key);
@@ -869,7 +869,8 @@ __global__ void __launch_bounds__(BX) k_aa_even(Geo g, S *__restrict__ a,
     const int X = blockIdx.x * BX + threadIdx.x + 1;
     const int Y = blockIdx.y + 1;
     if (pf_rows_aa_wide<S>() > 0 && threadIdx.x == 0)
-        prefetch_rows_l2<S, BX, 1>(g, a, 1 + BX * (int)blockIdx.x, Y + pf_rows_aa_wide<S>());
+        prefetch_rows_l2<S, BX, 1>(g, a, 1 + BX * (int)blockIdx.x, Y + pf_rows_aa_wide<S>(),
+                                   tag);
     if (X <= g.lx) aa_even_node<S>(g, a, tag, bc, omega, side, sc, inv, X, Y);
 }
 
@@ -882,7 +883,8 @@ __global__ void __launch_bounds__(BX) k_aa_odd(Geo g, S *__restrict__ a,
     const int X = blockIdx.x * BX + threadIdx.x + 1;
     const int Y = blockIdx.y + 1;
     if (pf_rows_aa_wide<S>() > 0 && threadIdx.x == 0)
-        prefetch_rows_l2<S, BX, 2>(g, a, 1 + BX * (int)blockIdx.x, Y + pf_rows_aa_wide<S>());
+        prefetch_rows_l2<S, BX, 2>(g, a, 1 + BX * (int)blockIdx.x, Y + pf_rows_aa_wide<S>(),
+                                   tag);
     if (X <= g.lx) aa_odd_node<S>(g, a, tag, bc, omega, side, sc, inv, X, Y);
 }
 
@@ -934,7 +936,8 @@ __global__ void __launch_bounds__(BX, SHIFT ? 7 : 8) k_aa4_even(Geo g, S *__rest
     using H = Half2Ops<S>;
     const int x0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x), Y = blockIdx.y + 1, lane = threadIdx.x & 31;
     if (LBGPU_PF_ROWS_AA > 0 && threadIdx.x == 0)
-        prefetch_rows_l2<S, 4 * BX, 1>(g, a, 1 + 4 * BX * (int)blockIdx.x, Y + LBGPU_PF_ROWS_AA);
+        prefetch_rows_l2<S, 4 * BX, 1>(g, a, 1 + 4 * BX * (int)blockIdx.x, Y + LBGPU_PF_ROWS_AA,
+                                       tag);
     const unsigned key = g.rs_key;
     if (!aa_quad_vec<S, SHIFT>(g, x0, Y, lane)) {
         for (int k = 0; k < 4; ++k)
@@ -964,7 +967,8 @@ __global__ void __launch_bounds__(BX, SHIFT ? 6 : 7) k_aa4_odd(Geo g, S *__restr
     using H = Half2Ops<S>;
     const int x0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x), Y = blockIdx.y + 1, lane = threadIdx.x & 31;
     if (LBGPU_PF_ROWS_AA > 0 && threadIdx.x == 0)
-        prefetch_rows_l2<S, 4 * BX, 2>(g, a, 1 + 4 * BX * (int)blockIdx.x, Y + LBGPU_PF_ROWS_AA);
+        prefetch_rows_l2<S, 4 * BX, 2>(g, a, 1 + 4 * BX * (int)blockIdx.x, Y + LBGPU_PF_ROWS_AA,
+                                       tag);
     const unsigned key = g.rs_key;
     if (!aa_quad_vec<S, SHIFT>(g, x0, Y, lane)) {
         for (int k = 0; k < 4; ++k)
