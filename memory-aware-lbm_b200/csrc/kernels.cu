@@ -12,7 +12,13 @@
 //   second buffer that is reused every other step).
 //
 // Storage types: double (exact FP64 arithmetic), float, __half / __nv_bfloat16 offsets
-// (codec.cuh), all with the same index space (layout.cuh).
+// (codec.cuh; optionally offset from a per-row equilibrium and stochastically rounded), all with
+// the same index space (layout.cuh).
+//
+// Memory system: the step kernels stream the lattice once per step from HBM; one thread a block
+// prefetches into L2 the rows a block a few rows further down will read
+// (cp.async.bulk.prefetch.L2, distances measured per kernel); the two-step sweep moves its next
+// row into shared memory with cp.async while it computes.
 #include <algorithm>
 #include "codec.cuh"
 #include "kernels.h"
