@@ -72,11 +72,11 @@ template <> struct Codec<__nv_bfloat16> {
 //   key_k = rs_key(seed, k)                              per collision (host), never 0
 //   H     = rs_mix((Y (lx + 2) + x0) ^ key_k)            per quad of nodes x0..x0+3 of a row,
 //                                                        x0 = X - ((X - 1) mod 4)
-//   h     = H * C_q,  q = X - x0                         per node, C_q odd
-//   r_i   = bits 16..31 of h * K_i                       per direction, K_i odd
-// One hash serves four nodes (the 16-bit kernels' unit of work); the two multiplies fold into
-// one by a constant there.  rs_mix is the 32-bit integer hash "lowbias32" (C. Wellons,
-// hash-prospector).
+//   P     = H * M(p, i),  p = (X - x0) / 2               per pair of nodes and direction, M odd
+//   node x0 + 2p takes bits 0..15 of P, node x0 + 2p + 1 bits 16..31
+// which is the operand layout of cvt.rs.f16x2: a quad's direction-i pair converts with P as
+// rbits as it is, one hash a quad and one multiply a stored pair.  rs_mix is the 32-bit integer
+// hash "lowbias32" (C. Wellons, hash-prospector).
 __host__ __device__ __forceinline__ unsigned rs_mix(unsigned x)
 {
     x ^= x >> 16;
@@ -93,40 +93,43 @@ __host__ __device__ __forceinline__ unsigned rs_key(unsigned seed, unsigned long
     return rs_mix(seed ^ rs_mix(lo ^ rs_mix(hi + 0x9e3779b9u))) | 1u;
 }
 
-__host__ __device__ __forceinline__ unsigned rs_place(unsigned hq, int q)
+__host__ __device__ __forceinline__ unsigned rs_pair(unsigned hq, int p, int i)
 {
-    return hq * (0x85ebca6bu + (unsigned)q * 0x3c6ef372u);   // odd for every q
+    return hq * (0x9e3779b9u * (unsigned)(2 * (9 * p + i) + 1));   // odd multiplier: a bijection of hq
 }
 
-__host__ __device__ __forceinline__ unsigned rs_dir(unsigned h, int i)
-{
-    return h * (0x9e3779b9u * (unsigned)(2 * i + 1));   // odd multiplier: a bijection of h
-}
+// A node's place in its quad and the quad's hash (RS kernels; zero otherwise).
+struct RsNode {
+    unsigned hq;
+    int q;
+};
 
 template <class S> struct RsOps;
 template <> struct RsOps<__half> {
-    // two values (lo -> bits 0..15, hi -> bits 16..31 of the result), random words rlo, rhi
-    static __device__ __forceinline__ unsigned pack(float lo, float hi, unsigned rlo, unsigned rhi)
+    // two values (lo -> bits 0..15 of the result with the random bits 0..15 of r, hi -> bits
+    // 16..31 with r's bits 16..31)
+    static __device__ __forceinline__ unsigned pack(float lo, float hi, unsigned r)
     {
         unsigned d;
-        asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(__byte_perm(rlo, rhi, 0x7632)));
+        asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(r));
         return d;
     }
+    // one value with the random bits 0..15 of r
     static __device__ __forceinline__ __half one(float v, unsigned r)
     {
-        return __ushort_as_half((unsigned short)(pack(v, 0.0f, r, 0u) & 0xffffu));
+        return __ushort_as_half((unsigned short)(pack(v, 0.0f, r & 0xffffu) & 0xffffu));
     }
 };
 template <> struct RsOps<__nv_bfloat16> {
-    static __device__ __forceinline__ unsigned pack(float lo, float hi, unsigned rlo, unsigned rhi)
+    static __device__ __forceinline__ unsigned pack(float lo, float hi, unsigned r)
     {
         unsigned d;
-        asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(__byte_perm(rlo, rhi, 0x7632)));
+        asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(r));
         return d;
     }
     static __device__ __forceinline__ __nv_bfloat16 one(float v, unsigned r)
     {
-        return __ushort_as_bfloat16((unsigned short)(pack(v, 0.0f, r, 0u) & 0xffffu));
+        return __ushort_as_bfloat16((unsigned short)(pack(v, 0.0f, r & 0xffffu) & 0xffffu));
     }
 };
 

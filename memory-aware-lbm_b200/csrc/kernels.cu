@@ -210,21 +210,24 @@ template <> struct Work<__nv_bfloat16> {
 // then never 0.
 // The random word of node (X, Y) for a collision key.
 template <class S, bool RS>
-__device__ __forceinline__ unsigned rs_node(const Geo &g, unsigned key, int X, int Y)
+__device__ __forceinline__ RsNode rs_node(const Geo &g, unsigned key, int X, int Y)
 {
     if constexpr (RS && sizeof(S) == 2) {
         const int q = (X - 1) & 3;
-        return rs_place(rs_mix(((unsigned)Y * (unsigned)(g.lx + 2) + (unsigned)(X - q)) ^ key), q);
+        return RsNode{rs_mix(((unsigned)Y * (unsigned)(g.lx + 2) + (unsigned)(X - q)) ^ key), q};
     }
-    return 0u;
+    return RsNode{0u, 0};
 }
 
 // A post-collision working value of direction i as stored: rounded to nearest, or (RS)
 // stochastically with the node's random word h.
 template <class S, bool RS>
-__device__ __forceinline__ S put(typename Work<S>::W w, int i, float sc, unsigned h)
+__device__ __forceinline__ S put(typename Work<S>::W w, int i, float sc, RsNode h)
 {
-    if constexpr (RS && sizeof(S) == 2) return RsOps<S>::one(w, rs_dir(h, i));
+    if constexpr (RS && sizeof(S) == 2) {
+        const unsigned p = rs_pair(h.hq, h.q >> 1, i);
+        return RsOps<S>::one(w, (h.q & 1) ? (p >> 16) : p);
+    }
     return Work<S>::store(w, i, sc);
 }
 
@@ -395,7 +398,7 @@ __global__ void __launch_bounds__(BX) k_collide_inplace(Geo g, S *__restrict__ b
 #pragma unroll
     for (int i = 0; i < 9; ++i) f[i] = Work<S>::load(plane(buf, g, i)[o], i, inv);
     collide_w<S>(bc, g, tag[o], X, Y, f, omega, sc, inv);
-    const unsigned h = rs_node<S, RS>(g, g.rs_key, X, Y);
+    const RsNode h = rs_node<S, RS>(g, g.rs_key, X, Y);
 #pragma unroll
     for (int i = 0; i < 9; ++i) plane(buf, g, i)[o] = put<S, RS>(stored_out<S>(g, Y, i, f[i], sc), i, sc, h);
     if (g.perimeter(X, Y)) {
@@ -493,7 +496,7 @@ __device__ __forceinline__ void pull_node(const Geo &g, const S *__restrict__ sr
         }
     }
     collide_w<S, SH>(bc, g, tag[o], X, Y, f, omega, sc, inv);
-    const unsigned h = rs_node<S, RS>(g, key, X, Y);
+    const RsNode h = rs_node<S, RS>(g, key, X, Y);
 #pragma unroll
     for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = put<S, RS>(stored_out<S, SH>(g, Y, i, f[i], sc), i, sc, h);
     if (edge) {
@@ -503,23 +506,21 @@ __device__ __forceinline__ void pull_node(const Geo &g, const S *__restrict__ sr
     }
 }
 
-// Random words of the quad's nodes x0..x0+3 (RS only).
+// The hash of the quad x0..x0+3 (RS only).
 template <class S, bool RS>
-__device__ __forceinline__ void quad_words(const Geo &g, unsigned key, int x0, int Y, unsigned h[4])
+__device__ __forceinline__ unsigned quad_hash(const Geo &g, unsigned key, int x0, int Y)
 {
-    const unsigned hq = RS ? rs_mix(((unsigned)Y * (unsigned)(g.lx + 2) + (unsigned)x0) ^ key) : 0u;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) h[k] = rs_place(hq, k);
+    return RS ? rs_mix(((unsigned)Y * (unsigned)(g.lx + 2) + (unsigned)x0) ^ key) : 0u;
 }
 
 // Direction i of a quad's four working values as the stored aligned word pair.
 template <class S, bool RS>
-__device__ __forceinline__ uint2 pack_quad(const float D[4][9], int i, const unsigned h[4])
+__device__ __forceinline__ uint2 pack_quad(const float D[4][9], int i, unsigned hq)
 {
     uint2 w;
     if constexpr (RS) {
-        w.x = RsOps<S>::pack(D[0][i], D[1][i], rs_dir(h[0], i), rs_dir(h[1], i));
-        w.y = RsOps<S>::pack(D[2][i], D[3][i], rs_dir(h[2], i), rs_dir(h[3], i));
+        w.x = RsOps<S>::pack(D[0][i], D[1][i], rs_pair(hq, 0, i));
+        w.y = RsOps<S>::pack(D[2][i], D[3][i], rs_pair(hq, 1, i));
     } else {
         w.x = Half2Ops<S>::pack(D[0][i], D[1][i]);
         w.y = Half2Ops<S>::pack(D[2][i], D[3][i]);
@@ -588,15 +589,14 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
         for (int k = 0; k < 4; ++k)
             collide_w<S, SHIFT ? 1 : 0>(bc, g, (int)((tq >> (8 * k)) & 0xff), x0 + k, Y, D[k], omega, sc, inv);
     }
-    unsigned h[4];
-    quad_words<S, RS>(g, key, x0, Y, h);
+    const unsigned hq = quad_hash<S, RS>(g, key, x0, Y);
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
         if (SHIFT) {
 #pragma unroll
             for (int k = 0; k < 4; ++k) D[k][i] = stored_out<S, 1>(g, Y, i, D[k][i], sc);
         }
-        *reinterpret_cast<uint2 *>(plane(dst, g, i) + o) = pack_quad<S, RS>(D, i, h);
+        *reinterpret_cast<uint2 *>(plane(dst, g, i) + o) = pack_quad<S, RS>(D, i, hq);
     }
 }
 
@@ -726,7 +726,7 @@ __global__ void __launch_bounds__(W + 2) k_sweep2(Geo g, const S *__restrict__ s
                 }
                 collide_w<S>(bc, g, tag[g.idx(X, Y1)], X, Y1, f, omega, sc, inv);
                 const int sl = (Y1 + 3) % 3;
-                const unsigned h = rs_node<S, RS>(g, g.rs_key, X, Y1);
+                const RsNode h = rs_node<S, RS>(g, g.rs_key, X, Y1);
 #pragma unroll
                 for (int i = 0; i < 9; ++i) r1[sl][i][k] = put<S, RS>(stored_out<S>(g, Y1, i, f[i], sc), i, sc, h);
                 if (edge && X >= x0 && X < x0 + W && Y1 >= y0 && Y1 < yend) {
@@ -753,7 +753,7 @@ __global__ void __launch_bounds__(W + 2) k_sweep2(Geo g, const S *__restrict__ s
             }
             const long long o = g.idx(X, Y2);
             collide_w<S>(bc, g, tag[o], X, Y2, f, omega, sc, inv);
-            const unsigned h = rs_node<S, RS>(g, g.rs_key2, X, Y2);
+            const RsNode h = rs_node<S, RS>(g, g.rs_key2, X, Y2);
 #pragma unroll
             for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = put<S, RS>(stored_out<S>(g, Y2, i, f[i], sc), i, sc, h);
             if (edge) {
@@ -818,7 +818,7 @@ __device__ __forceinline__ void aa_even_node(const Geo &g, S *__restrict__ a, co
         }
     }
     collide_w<S, SH>(bc, g, tag[o], X, Y, f, omega, sc, inv);
-    const unsigned h = rs_node<S, RS>(g, key, X, Y);
+    const RsNode h = rs_node<S, RS>(g, key, X, Y);
 #pragma unroll
     for (int i = 0; i < 9; ++i) plane(a, g, opp(i))[o] = put<S, RS>(stored_out<S, SH>(g, Y, i, f[i], sc), i, sc, h);
     if (edge) {
@@ -855,7 +855,7 @@ __device__ __forceinline__ void aa_odd_node(const Geo &g, S *__restrict__ a, con
         }
     }
     collide_w<S, SH>(bc, g, tag[o], X, Y, f, omega, sc, inv);
-    const unsigned h = rs_node<S, RS>(g, key, X, Y);
+    const RsNode h = rs_node<S, RS>(g, key, X, Y);
 #pragma unroll
     for (int i = 0; i < 9; ++i)
         plane(a, g, i)[o + cx(i) + (long long)cy(i) * g.pitch] = put<S, RS>(stored_out<S, SH>(g, Y, i, f[i], sc), i, sc, h);
@@ -959,10 +959,9 @@ __global__ void __launch_bounds__(BX, SHIFT ? 7 : 8) k_aa4_even(Geo g, S *__rest
         D[2][i] = H::lo(v.y); D[3][i] = H::hi(v.y);
     }
     aa_collide_quad<S, SHIFT>(g, tag, bc, omega, sc, inv, x0, Y, o, D);
-    unsigned h[4];
-    quad_words<S, RS>(g, key, x0, Y, h);
+    const unsigned hq = quad_hash<S, RS>(g, key, x0, Y);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) *reinterpret_cast<uint2 *>(plane(a, g, opp(i)) + o) = pack_quad<S, RS>(D, i, h);
+    for (int i = 0; i < 9; ++i) *reinterpret_cast<uint2 *>(plane(a, g, opp(i)) + o) = pack_quad<S, RS>(D, i, hq);
 }
 
 template <class S, bool SHIFT, bool RS>
@@ -1001,8 +1000,7 @@ __global__ void __launch_bounds__(BX, SHIFT ? 6 : 7) k_aa4_odd(Geo g, S *__restr
         D[2][i] = H::lo(w1); D[3][i] = H::hi(w1);
     }
     aa_collide_quad<S, SHIFT>(g, tag, bc, omega, sc, inv, x0, Y, o, D);
-    unsigned hw[4];
-    quad_words<S, RS>(g, key, x0, Y, hw);
+    const unsigned hw = quad_hash<S, RS>(g, key, x0, Y);
 #pragma unroll
     for (int i = 0; i < 9; ++i) {    // direction i scattered to the natural slots of x + c_i
         const uint2 wq = pack_quad<S, RS>(D, i, hw);
