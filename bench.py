@@ -309,6 +309,24 @@ def time_lattice(lbgpu, nx, ny, precision, scheme, steps, warmup, dist, sampler_
         lat.close()
 
 
+def step_kernel(precision, scheme):
+    """The kernel that does a step of this storage and scheme (its name in the ncu launch list)."""
+    half = lbgpu_storage_base(precision) in ("f16", "bf16")
+    if scheme == "pull2":
+        return "k_sweep2"
+    if scheme == "aa":
+        return "k_aa4_even/k_aa4_odd" if half else "k_aa_even/k_aa_odd"
+    return "k_pull4h" if half else "k_pull"
+
+
+def lbgpu_storage_base(precision):
+    """'f16sr' -> 'f16' without importing the library (used for labels only)."""
+    for base in ("bf16", "f16", "f32", "f64"):
+        if precision.startswith(base):
+            return base
+    return precision
+
+
 def run_ours(args, dist):
     import lbgpu
 
@@ -393,8 +411,7 @@ def run_ours(args, dist):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
                      "traffic": None if traffic is None else int(traffic),
-                     "kernel": f"k_pull ({args.precision})" if args.scheme == "pull" else
-                               f"k_aa ({args.precision})",
+                     "kernel": f"{step_kernel(args.precision, args.scheme)} ({args.precision})",
                      "bytes_per_update": bpu, "peak_kind": f"{peak_kind} hbm_gbs (copy)"},
         "cpu_baseline": cpu,
         "e2e": e2e,
