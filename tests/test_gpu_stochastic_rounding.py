@@ -235,3 +235,26 @@ def test_batch_members_round_like_the_lattice_alone(precision, shape):
     finally:
         for lat in lats:
             lat.close()
+
+
+@pytest.mark.parametrize("precision", ["f16", "bf16"])
+def test_stochastic_rounding_with_the_extrapolated_outlet(precision):
+    """The reference driver's outlet (zero-gradient density pass before every step): pull and AA
+    stay bit-identical, and the two-step setting falls back to single steps with the same bits."""
+    lx, ly, n = 260, 41, 31
+
+    def run(scheme, sweep=1):
+        with lbgpu.Lattice(lx, ly, precision, scheme) as lat:
+            lat.set_offset_scale(SCALE[precision])
+            lat.set_stochastic_rounding(True, 9)
+            lat.setup_cylinder(lx // 4, ly // 2, ly // 10 + 1, 0.03, 60.0, lbgpu.WALL_REGULARIZED,
+                               lbgpu.OUTLET_ZGB)
+            if sweep == 2:
+                lat.set_sweep_steps(2)
+            lat.step(n)
+            return lat.populations()
+
+    ref = run("pull")
+    aa, two = run("aa"), run("pull", 2)
+    assert same(aa, ref), describe_diff(aa, ref)
+    assert same(two, ref), describe_diff(two, ref)
