@@ -96,7 +96,9 @@ void collide_tight_panel_ix(Simulation *sim);
 void collide_tight_panel_iy(Simulation *sim);
 void collide_tight_panel_iy_openmp(Simulation *sim);
 
-/* Construction (reference lb.h:125-127, lb.c:85-121). */
+/* Construction (reference lb.h:125-127, lb.c:85-121).  constructSim accepts
+ * 1 <= lx <= LBGPU_MAX_LX and 1 <= ly <= LBGPU_MAX_LY (lbgpu.h: 2^20 and 65533, CUDA's grid
+ * limit); other sizes leave *sim zeroed and record LB_ERR_ARG. */
 void constructSim(Simulation *sim, int lx, int ly);
 void destructSim(Simulation *sim);
 void setDynamics(Simulation *sim, int iX, int iY, Dynamics *dyn);

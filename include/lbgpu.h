@@ -100,7 +100,10 @@ int lbgpu_set_device(int device);
 int lbgpu_device_count(void);
 
 /* Allocate a lattice on the current CUDA device: two population buffers for
- * LBGPU_PULL, one for LBGPU_AA, plus tags and tables. */
+ * LBGPU_PULL, one for LBGPU_AA, plus tags and tables.  1 <= lx <= LBGPU_MAX_LX and
+ * 1 <= ly <= LBGPU_MAX_LY, else LB_ERR_ARG: the row-wise kernels launch one grid row per
+ * lattice row including the two ghost rows, and CUDA allows at most 65535 grid rows. */
+enum { LBGPU_MAX_LX = 1 << 20, LBGPU_MAX_LY = 65533 };
 int lbgpu_create(int lx, int ly, int precision, int scheme, lbgpu_lattice **out);
 int lbgpu_destroy(lbgpu_lattice *lat);
 
@@ -178,8 +181,9 @@ int lbgpu_get_macros(lbgpu_lattice *lat, double *rho, double *ux, double *uy);
  * the reference.  Allocates nothing: the device scratch is a fixed array of 3 x 262,144
  * doubles (6 MiB, held by every GPU that loads the library), so lattices above 262,144
  * interior nodes get LB_ERR_CAPACITY.  The first call on a device looks up that array's
- * address; make it before any stream capture.  All calls share the array: calls that overlap
- * on the GPU race. */
+ * address; make it before any stream capture.  Later calls look it up again unless the
+ * lattice's stream is capturing, so a device reset (cudaDeviceReset) between calls is safe.
+ * All calls share the array: calls that overlap on the GPU race. */
 int lbgpu_get_macros_noalloc(lbgpu_lattice *lat, double *rho, double *ux, double *uy);
 
 /* FP64 sums over the current state, computed on the device in a fixed order (bitwise

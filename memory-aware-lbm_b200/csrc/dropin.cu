@@ -406,7 +406,11 @@ void constructSim(Simulation *sim, int lx, int ly)
 {
     if (!sim) { set_error(LB_ERR_ARG, "constructSim: null simulation"); return; }
     std::memset(sim, 0, sizeof *sim);
-    if (lx < 1 || ly < 1) { set_error(LB_ERR_ARG, "constructSim: size %d x %d", lx, ly); return; }
+    if (lx < 1 || ly < 1 || lx > LBGPU_MAX_LX || ly > LBGPU_MAX_LY) {
+        set_error(LB_ERR_ARG, "constructSim: size %d x %d out of range (1..%d x 1..%d)", lx, ly,
+                  LBGPU_MAX_LX, LBGPU_MAX_LY);
+        return;
+    }
     const size_t nodes = (size_t)(lx + 2) * (ly + 2);
     sim->lx = lx;
     sim->ly = ly;

@@ -60,8 +60,11 @@ static size_t elem_bytes(int precision)
 
 int Lattice::create(int lx_, int ly_, int precision_, int scheme_)
 {
-    if (lx_ < 1 || ly_ < 1 || lx_ > (1 << 20) || ly_ > (1 << 20))
-        return set_error(LB_ERR_ARG, "lattice size %d x %d out of range", lx_, ly_);
+    // The row-wise kernels launch one grid row per lattice row, ghost rows included, and CUDA
+    // caps gridDim.y at 65535: hence ly <= LBGPU_MAX_LY.
+    if (lx_ < 1 || ly_ < 1 || lx_ > LBGPU_MAX_LX || ly_ > LBGPU_MAX_LY)
+        return set_error(LB_ERR_ARG, "lattice size %d x %d out of range (1..%d x 1..%d)", lx_, ly_,
+                         LBGPU_MAX_LX, LBGPU_MAX_LY);
     if (precision_ < LBGPU_F64 || precision_ > LBGPU_BF16)
         return set_error(LB_ERR_ARG, "unknown precision %d", precision_);
     if (scheme_ != LBGPU_PULL && scheme_ != LBGPU_AA)
@@ -293,6 +296,7 @@ size_t Lattice::stage_cols(int rs) const
     size_t cols = ((size_t)64 << 20) / col;
     if (cols < 1) cols = 1;
     if (cols > (size_t)(lx + 2)) cols = (size_t)(lx + 2);
+    if (cols > kMaxGridY) cols = kMaxGridY;   // one grid row a column in the copy kernels
     return cols;
 }
 
@@ -319,6 +323,7 @@ int Lattice::upload_record_rows(int b, const double *host, int rs, int X0, int X
     size_t cols = ((size_t)64 << 20) / (band * sizeof(double));
     if (cols < 1) cols = 1;
     if (cols > (size_t)(X1 - X0)) cols = (size_t)(X1 - X0);
+    if (cols > kMaxGridY) cols = kMaxGridY;
     LB_TRY(ensure_stage(cols * band * sizeof(double)));
     for (int c0 = X0; c0 < X1; c0 += (int)cols) {
         const int c1 = (c0 + (int)cols < X1) ? c0 + (int)cols : X1;

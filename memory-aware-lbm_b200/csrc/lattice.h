@@ -17,6 +17,9 @@ void clear_error();
 
 enum { FORM_L = 0, FORM_C = 1 };
 
+// CUDA's limit on gridDim.y (kernels that launch one grid row a lattice row or column).
+constexpr size_t kMaxGridY = 65535;
+
 struct Lattice {
     int lx = 0, ly = 0;
     int precision = 0;   // LBGPU_F64 / F32 / F16 / BF16

@@ -14,9 +14,12 @@
 // interior nodes are rejected with LB_ERR_CAPACITY (use lbgpu_get_macros for those).
 //
 // Set-up: the first call on each device looks up the array's device address with
-// cudaGetSymbolAddress while that device is current and keeps it for later calls; make that
-// first call before any stream capture.  Host code never uses the array's name as an address:
-// on the host it names a stand-in, not device memory.
+// cudaGetSymbolAddress while that device is current; make that first call before any stream
+// capture.  Calls made while the lattice's stream is not capturing look the address up again
+// (a host application that resets the device with cudaDeviceReset reloads the library's device
+// code, and the array with it, at a new address); calls made during a capture use the address
+// the last uncaptured call found.  Host code never uses the array's name as an address: on the
+// host it names a stand-in, not device memory.
 //
 // Sharing: all calls use the same array, which keeps the last call's contents.  Nothing in it
 // has to start at zero: every element a call copies back was written by that same call.  Calls
@@ -36,14 +39,21 @@ __device__ __align__(256) double g_macros_scratch[3 * kMaxNodes];
 double *g_scratch_addr[kMaxDevices];
 std::mutex g_scratch_mu;
 
-// Device address of g_macros_scratch on the current device (looked up once per device).
-int scratch_address(int dev, double **out)
+// Device address of g_macros_scratch on the current device: looked up afresh unless `stream`
+// is capturing, in which case the address of the last uncaptured call on the device is used.
+int scratch_address(int dev, cudaStream_t stream, double **out)
 {
     if (dev < 0 || dev >= kMaxDevices)
         return lbgpu::set_error(LB_ERR_CAPACITY, "lbgpu_get_macros_noalloc: device %d beyond %d",
                                 dev, kMaxDevices);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (int rc = lbgpu::cuda_error(cudaStreamIsCapturing(stream, &cap), "cudaStreamIsCapturing"))
+        return rc;
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
+    if (cap != cudaStreamCaptureStatusNone && !g_scratch_addr[dev])
+        return lbgpu::set_error(LB_ERR_STATE, "lbgpu_get_macros_noalloc: the first call on device "
+                                "%d must come before any stream capture", dev);
+    if (cap == cudaStreamCaptureStatusNone) {
         void *p = nullptr;
         if (int rc = lbgpu::cuda_error(cudaGetSymbolAddress(&p, g_macros_scratch),
                                        "cudaGetSymbolAddress(macros scratch)"))
@@ -71,7 +81,7 @@ extern "C" int lbgpu_get_macros_noalloc(lbgpu_lattice *h, double *rho, double *u
     if (prev != L.device)
         if (int rc = lbgpu::cuda_error(cudaSetDevice(L.device), "cudaSetDevice")) return rc;
     double *s = nullptr;
-    int rc = scratch_address(L.device, &s);
+    int rc = scratch_address(L.device, L.stream, &s);
     if (rc == LB_OK) {
         int v, par;
         L.view(v, par);

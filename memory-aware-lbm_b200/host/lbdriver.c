@@ -173,7 +173,10 @@ int lbdrv_run(const lbdrv_config *c, int nsteps, double *out, double *seconds)
     }
     lbClearError();
     ch = channel_build(c);
-    if (!ch) return -LB_ERR_ALLOC;
+    if (!ch) {   /* constructSim records why (a size out of range, no host memory) */
+        rc = lbGetLastError();
+        return -(rc ? rc : LB_ERR_ALLOC);
+    }
     t0 = now_s();
     for (t = 0; t < nsteps; t += two ? 2 : 1) {
         if (c->outlet == LBGPU_OUTLET_ZGB) zgb_update(ch);

@@ -54,7 +54,7 @@ def test_library_exports_driver_globals():
         ctypes.c_int.in_dll(L, name)   # raises ValueError when absent
 
 
-def test_struct_layouts_match_the_reference_abi():
+def test_struct_layouts_match_the_reference_abi(tmp_path):
     # Node = 9 doubles + pointer (80 bytes), Dynamics = 2 pointers, BC data = ptr + 2 doubles
     src = r"""
 #include <stdio.h>
@@ -66,8 +66,7 @@ int main(void) {
          sizeof(PressureBCData), offsetof(Simulation, lattice), offsetof(Simulation, tmpLattice));
   return 0; }
 """
-    exe = os.path.join(ROOT, "_work", "abi_layout")
-    os.makedirs(os.path.dirname(exe), exist_ok=True)
+    exe = str(tmp_path / "abi_layout")
     cfile = exe + ".c"
     with open(cfile, "w") as f:
         f.write(src)
@@ -163,8 +162,18 @@ def test_bad_arguments_are_rejected():
     lbgpu.clear_error()
     assert L.lbgpu_create(8, 8, 9, 0, ctypes.byref(h)) == 3
     lbgpu.clear_error()
+    # CUDA's 65535 grid rows bound ly (one grid row a lattice row, two ghost rows included)
+    assert L.lbgpu_create(16, 65534, 0, 0, ctypes.byref(h)) == 3
+    assert "65533" in lbgpu.last_error()[1]
+    lbgpu.clear_error()
+    assert L.lbgpu_create((1 << 20) + 1, 8, 0, 0, ctypes.byref(h)) == 3
+    lbgpu.clear_error()
     with pytest.raises(lbgpu.LbError) as e:
         lbgpu.drive(-1, 10, 5, 6, 2, 2, "origin")
+    assert e.value.code == 3
+    lbgpu.clear_error()
+    with pytest.raises(lbgpu.LbError) as e:
+        lbgpu.drive(16, 65534, 5, 6, 2, 2, "origin", want_lattice=False)
     assert e.value.code == 3
     lbgpu.clear_error()
     s = ctypes.c_void_p()

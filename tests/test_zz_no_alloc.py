@@ -71,3 +71,27 @@ def test_noalloc_rejects_lattices_beyond_the_fixed_scratch():
         # the allocating entry point still serves it
         rho, _, _ = lat.macros()
         assert rho.shape == (512, 1024) and np.isfinite(rho).all()
+
+
+def test_noalloc_readout_at_exactly_the_fixed_scratch_size():
+    # 512 x 512 = 262,144 interior nodes: the largest lattice the fixed array serves
+    with _lattice(O.Cylinder.baseline(512, 512), 12) as lat:
+        want = lat.macros()
+        a = lat.macros_noalloc()
+        b = lat.macros_noalloc()
+    for w, x, y in zip(want, a, b):
+        assert np.array_equal(_bits(w), _bits(x))
+        assert np.array_equal(_bits(w), _bits(y))
+
+
+def test_noalloc_readout_of_density_only():
+    # any output pointer may be NULL: ask for rho alone, twice
+    c = O.Cylinder.reference_driver(200, 90)
+    with _lattice(c, 30) as lat:
+        want, _, _ = lat.macros()
+        for _ in range(2):
+            rho = np.zeros(c.lx * c.ly)
+            rc = lbgpu.lib().lbgpu_get_macros_noalloc(lat.h, rho.ctypes.data_as(lbgpu._dp),
+                                                      None, None)
+            assert rc == 0, lbgpu.last_error()
+            assert np.array_equal(_bits(want.reshape(-1)), _bits(rho))
