@@ -209,6 +209,12 @@ def cylinder(nx, ny):
     return nx // 5 + 1, ny // 2 + 1, ny // 10 + 1
 
 
+def workload(nx, ny):
+    """The workload label both arms print."""
+    return (f"cylinder channel {nx}x{ny} ({nx * ny / 1e6:.1f}M nodes), Re=100, uMax=0.02, "
+            f"bounce-back walls, constant-density outlet")
+
+
 # ---------------------------------------------------------------------------------------
 # the reference's own CPU code (oracle/_ref) on this host
 # ---------------------------------------------------------------------------------------
@@ -267,7 +273,7 @@ def run_reference_arm(args, dist):
         "n_gpus": args.gpus, "steps": r["steps"], "warmup": args.warmup,
         "ms_per_step": round(1e3 * r["seconds"] / r["steps"], 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"cylinder channel {nx}x{ny}, Re=100, uMax=0.02, FP64",
+        "config": {"workload": workload(nx, ny), "kernel": f"reference {r['variant']} (FP64)",
                    "nodes": nx * ny, "variant": r["variant"], "parallelism": "openmp",
                    "l2": "inputs larger than L2"},
         "cpu_baseline": {"value": round(r["mlups"], 2), "unit": "MLUPS", "cores": r["threads"],
@@ -379,9 +385,10 @@ def run_ours(args, dist):
         _, done, secs = lbgpu.drive(nx, ny, ox, oy, r, K, "combine", wall=lbgpu.WALL_BOUNCEBACK,
                                     outlet=lbgpu.OUTLET_CONST, sync="outlet", want_lattice=False)
         secs = dist.max(secs)
-        node_bytes = 80 * (nx + 2) * (ny + 2)
-        h2d = 2 * node_bytes + 8 * (nx + 2) * (ny + 2)      # both host arrays + dynamics map
-        d2h = node_bytes + done * 2 * 80 * (ny + 2)          # final copy + two columns a step
+        # bytes the library copied (lbdrv_last_transfer_bytes): the first call's upload of the
+        # current lattice, the second buffer's ghost ring and perimeter bands, the dynamics tags
+        # and tables; the outlet columns after every step; the final copy-back
+        h2d, d2h = lbgpu.drive_transfer_bytes()
         e2e = {"value": round(dist.world * nodes * done / secs / 1e6, 1), "unit": "MLUPS",
                "h2d_bytes_per_step": int(h2d / done), "d2h_bytes_per_step": int(d2h / done),
                "seconds": round(secs, 3), "steps": done,
@@ -403,8 +410,9 @@ def run_ours(args, dist):
         "metric": "MLUPS", "value": round(mlups, 1), "unit": "MLUPS", "n_gpus": dist.world,
         "steps": K, "warmup": W, "ms_per_step": round(ms / K, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
-        "config": {"workload": f"cylinder channel {nx}x{ny} ({nodes / 1e6:.1f}M nodes), Re=100, uMax=0.02, "
-                               f"{args.precision.upper()} {args.scheme} kernel",
+        "config": {"workload": workload(nx, ny),
+                   "kernel": f"{step_kernel(args.precision, args.scheme)} "
+                             f"({args.precision.upper()} {args.scheme})",
                    "nodes_per_gpu": nodes, "l2": "inputs larger than L2 (lattice "
                    f"{bpu * nodes / 1e9:.1f} GB streamed per step)",
                    "parallelism": f"replicas x{dist.world}"},

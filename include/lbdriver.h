@@ -30,6 +30,10 @@ typedef struct {
  * *seconds.  Returns the number of steps run, or -LB_ERR_* on failure. */
 int lbdrv_run(const lbdrv_config *cfg, int nsteps, double *out, double *seconds);
 
+/* Bytes copied host->device and device->host by the calling thread's last lbdrv_run, from
+ * its first step through the final copy-back (lbGetTransferBytes of its simulation). */
+void lbdrv_last_transfer_bytes(unsigned long long *h2d, unsigned long long *d2h);
+
 /* Steps advanced by one call of the variant's collision function (1 or 2). */
 int lbdrv_variant_steps(int variant);
 

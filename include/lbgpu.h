@@ -71,6 +71,11 @@ void lbSyncToHost(Simulation *sim);
  * entry point.  (setDynamics marks the dynamics dirty by itself.) */
 void lbMarkHostDirty(Simulation *sim);
 
+/* Bytes the library has copied host->device and device->host for this simulation since
+ * constructSim (populations, dynamics, tables, outlet columns, read-outs).  No counterpart in
+ * the reference: it lets a benchmark declare the transfers of the drop-in path. */
+void lbGetTransferBytes(const Simulation *sim, unsigned long long *h2d, unsigned long long *d2h);
+
 /* ---- lattice object ------------------------------------------------------------------ */
 enum { LBGPU_F64 = 0, LBGPU_F32 = 1, LBGPU_F16 = 2, LBGPU_BF16 = 3 };
 enum { LBGPU_PULL = 0, LBGPU_AA = 1 };

@@ -219,6 +219,7 @@ int upload_dynp(DropIn *c)
     if (int rc = lbgpu::cuda_error(cudaMemcpyAsync(c->dynp_dev, c->dynp.data(), bytes,
                                                    cudaMemcpyHostToDevice, c->L.stream), "upload dynamics pointers"))
         return rc;
+    c->L.h2d_bytes += bytes;
     if (int rc = lbgpu::cuda_error(cudaStreamSynchronize(c->L.stream), "upload dynamics pointers")) return rc;
     c->dynp_dirty = false;
     return LB_OK;
@@ -384,6 +385,7 @@ void two_steps(Simulation *sim, const char *fn, int need_x, int need_y)
                                               L.stream), fn) ||
             lbgpu::cuda_error(cudaStreamSynchronize(L.stream), fn))
             return;
+        L.d2h_bytes += zr.size() * 8;
         for (int k = 1; k <= sim->ly - 1; ++k) {
             if (myrho1) myrho1[k] = zr[2 * k];
             if (myrho2 && sim->lx >= 3) myrho2[k] = zr[2 * k + 1];
@@ -601,6 +603,13 @@ void lbSyncToHost(Simulation *sim)
     if (upload_dynp(c) != LB_OK) return;
     c->L.readout_records(reinterpret_cast<double *>(chunk_of(sim->lattice)), 10, c->dynp_dev, 0,
                          sim->lx + 2);
+}
+
+void lbGetTransferBytes(const Simulation *sim, unsigned long long *h2d, unsigned long long *d2h)
+{
+    DropIn *c = sim ? static_cast<DropIn *>(sim->device) : nullptr;
+    if (h2d) *h2d = (c && c->created) ? c->L.h2d_bytes : 0;
+    if (d2h) *d2h = (c && c->created) ? c->L.d2h_bytes : 0;
 }
 
 void lbMarkHostDirty(Simulation *sim)

@@ -310,6 +310,7 @@ int Lattice::upload_records(int b, const double *host, int rs, int X0, int X1)
         LB_CUDA(cudaMemcpyAsync(stage, host + (size_t)(c0 - X0) * col,
                                 (size_t)(c1 - c0) * col * sizeof(double),
                                 cudaMemcpyHostToDevice, stream), "upload populations");
+        h2d_bytes += (size_t)(c1 - c0) * col * sizeof(double);
         launch_upload(d, b, stage, rs, c0, c1, 0, ly + 2, stream);
         ++launches;
     }
@@ -330,6 +331,7 @@ int Lattice::upload_record_rows(int b, const double *host, int rs, int X0, int X
         LB_CUDA(cudaMemcpy2DAsync(stage, band * sizeof(double), host + (size_t)(c0 - X0) * col + (size_t)Y0 * rs,
                                   col * sizeof(double), band * sizeof(double), (size_t)(c1 - c0),
                                   cudaMemcpyHostToDevice, stream), "upload population rows");
+        h2d_bytes += (size_t)(c1 - c0) * band * sizeof(double);
         launch_upload(d, b, stage, rs, c0, c1, Y0, H, stream);
         ++launches;
     }
@@ -360,6 +362,7 @@ int Lattice::readout_records(double *host, int rs, const uint64_t *dynp_dev, int
         LB_CUDA(cudaMemcpyAsync(host + (size_t)(c0 - X0) * col, stage,
                                 (size_t)(c1 - c0) * col * sizeof(double),
                                 cudaMemcpyDeviceToHost, stream), "download populations");
+        d2h_bytes += (size_t)(c1 - c0) * col * sizeof(double);
     }
     LB_CUDA(cudaStreamSynchronize(stream), "readout");
     return check("readout");
@@ -392,6 +395,7 @@ int Lattice::get_macros(double *rho, double *ux, double *uy)
     if (rc == LB_OK && ux) rc = cuda_error(cudaMemcpyAsync(ux, dev + nn, nn * 8, cudaMemcpyDeviceToHost, stream), "macros");
     if (rc == LB_OK && uy) rc = cuda_error(cudaMemcpyAsync(uy, dev + 2 * nn, nn * 8, cudaMemcpyDeviceToHost, stream), "macros");
     if (rc == LB_OK) rc = cuda_error(cudaStreamSynchronize(stream), "macros");
+    d2h_bytes += nn * 8 * ((rho != nullptr) + (ux != nullptr) + (uy != nullptr));
     cudaFree(dev);
     return rc;
 }
@@ -409,6 +413,7 @@ int Lattice::moments(double out[8])
     launch_moments(d, v, cur, par, red_scratch, res, stream);
     LB_TRY(check("moments"));
     LB_CUDA(cudaMemcpyAsync(out, res, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream), "moments");
+    d2h_bytes += 8 * sizeof(double);
     LB_CUDA(cudaStreamSynchronize(stream), "moments");
     return LB_OK;
 }
@@ -438,6 +443,7 @@ int Lattice::velocity_average(double *ux, double *uy, long long *samples)
     if (ux) LB_CUDA(cudaMemcpyAsync(ux, vel_acc, nn * 8, cudaMemcpyDeviceToHost, stream), "velocity average");
     if (uy) LB_CUDA(cudaMemcpyAsync(uy, vel_acc + nn, nn * 8, cudaMemcpyDeviceToHost, stream), "velocity average");
     LB_CUDA(cudaStreamSynchronize(stream), "velocity average");
+    d2h_bytes += nn * 8 * ((ux != nullptr) + (uy != nullptr));
     const double k = 1.0 / (double)vel_samples;
     for (size_t i = 0; i < nn; ++i) {
         if (ux) ux[i] *= k;
@@ -451,6 +457,7 @@ int Lattice::upload_bc(const double *bc)
     std::memcpy(bc_host.data(), bc, bc_host.size() * sizeof(double));
     LB_CUDA(cudaMemcpyAsync(d.bc, bc_host.data(), bc_host.size() * sizeof(double),
                             cudaMemcpyHostToDevice, stream), "upload tables");
+    h2d_bytes += bc_host.size() * sizeof(double);
     // the copy reads bc_host asynchronously: wait so the caller may reuse its array and
     // the next refresh may overwrite bc_host
     LB_CUDA(cudaStreamSynchronize(stream), "upload tables");
@@ -463,6 +470,7 @@ int Lattice::upload_zgb_src(const int *src)
     LB_CUDA(cudaMemcpyAsync(const_cast<int *>(d.zgb_src), zgb_src_host.data(),
                             zgb_src_host.size() * sizeof(int), cudaMemcpyHostToDevice, stream),
             "upload zgb slots");
+    h2d_bytes += zgb_src_host.size() * sizeof(int);
     LB_CUDA(cudaStreamSynchronize(stream), "upload zgb slots");
     return LB_OK;
 }
@@ -471,6 +479,7 @@ int Lattice::upload_tag_plane(const uint8_t *plane)
 {
     LB_CUDA(cudaMemcpyAsync(const_cast<uint8_t *>(d.tag), plane, (size_t)d.g.plane,
                             cudaMemcpyHostToDevice, stream), "upload tags");
+    h2d_bytes += (size_t)d.g.plane;
     LB_CUDA(cudaStreamSynchronize(stream), "upload tags");
     return LB_OK;
 }
@@ -495,6 +504,7 @@ int Lattice::upload_tags_xy(const uint8_t *tag_xy)
     const size_t n = (size_t)(lx + 2) * (ly + 2);
     LB_TRY(ensure_stage(n));
     LB_CUDA(cudaMemcpyAsync(stage, tag_xy, n, cudaMemcpyHostToDevice, stream), "upload tags");
+    h2d_bytes += n;
     launch_tags_from_xy(d, reinterpret_cast<const uint8_t *>(stage), stream);
     LB_TRY(check("tags"));
     LB_CUDA(cudaStreamSynchronize(stream), "upload tags");

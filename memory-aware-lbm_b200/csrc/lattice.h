@@ -36,6 +36,7 @@ struct Lattice {
     cudaStream_t stream = nullptr;
     size_t bytes = 0;
     int launches = 0;    // kernels launched by the last public call
+    unsigned long long h2d_bytes = 0, d2h_bytes = 0;  // bytes copied host<->device so far
     int device = 0;      // CUDA device the lattice lives on
 
     std::vector<double> bc_host;   // [16*nb] last uploaded boundary tables

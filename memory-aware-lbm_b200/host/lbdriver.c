@@ -150,6 +150,14 @@ static Channel *channel_build(const lbdrv_config *c)
     return ch;
 }
 
+static __thread unsigned long long g_h2d, g_d2h;
+
+void lbdrv_last_transfer_bytes(unsigned long long *h2d, unsigned long long *d2h)
+{
+    if (h2d) *h2d = g_h2d;
+    if (d2h) *d2h = g_d2h;
+}
+
 int lbdrv_variant_steps(int variant)
 {
     return (variant >= LBDRV_TIGHT) ? 2 : 1;
@@ -172,6 +180,7 @@ int lbdrv_run(const lbdrv_config *c, int nsteps, double *out, double *seconds)
     default: return -LB_ERR_ARG;
     }
     lbClearError();
+    g_h2d = g_d2h = 0;
     ch = channel_build(c);
     if (!ch) {   /* constructSim records why (a size out of range, no host memory) */
         rc = lbGetLastError();
@@ -187,6 +196,7 @@ int lbdrv_run(const lbdrv_config *c, int nsteps, double *out, double *seconds)
     }
     lbSyncToHost(&ch->sim);
     t1 = now_s();
+    lbGetTransferBytes(&ch->sim, &g_h2d, &g_d2h);
     if (seconds) *seconds = t1 - t0;
     rc = lbGetLastError();
     if (out && rc == LB_OK)

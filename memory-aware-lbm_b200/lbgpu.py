@@ -147,6 +147,7 @@ def lib():
     L.lbgpu_last_kernel_launches.argtypes = [_vp]
     L.lbdrv_run.argtypes = [ctypes.POINTER(DriverConfig), ctypes.c_int, _dp,
                             ctypes.POINTER(ctypes.c_double)]
+    L.lbdrv_last_transfer_bytes.argtypes = [ctypes.POINTER(ctypes.c_ulonglong)] * 2
     L.computeMacros.argtypes = [_dp, _dp, _dp, _dp]
     L.computeEquilibrium.restype = ctypes.c_double
     L.computeEquilibrium.argtypes = [ctypes.c_int] + [ctypes.c_double] * 4
@@ -392,6 +393,13 @@ def drive(lx, ly, obst_x, obst_y, obst_r, nsteps, variant="origin", umax=0.02, r
         clear_error()
         raise LbError(-done, msg)
     return (out.reshape(lx + 2, ly + 2, 9) if out is not None else None), done, secs.value
+
+
+def drive_transfer_bytes():
+    """(host->device, device->host) bytes the calling thread's last drive() copied."""
+    a, b = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+    lib().lbdrv_last_transfer_bytes(ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value
 
 
 def declared_functions():

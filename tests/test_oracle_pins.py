@@ -6,6 +6,8 @@ These tests re-run the oracle restatement (oracle/lbm_oracle.c) on the same inpu
 bit-identical populations; where the reference build (oracle/_ref) is present they also run it
 live.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -101,3 +103,24 @@ def test_oracle_planted_mistake_is_caught():
     ref = O.run_reference(c, "origin", 50)
     st.omega = np.nextafter(st.omega, 2.0)
     assert not same(O.run(st, 50).lat, ref)
+
+
+_PERIODIC_REF = os.path.join(os.path.dirname(O.HERE), "oracle", "_ref", "periodic_ref")
+
+
+@pytest.mark.skipif(not os.path.exists(_PERIODIC_REF), reason="oracle/_ref/periodic_ref not built")
+def test_reference_periodic_driver_conserves_mass(tmp_path):
+    """The periodic-box driver's wrap (the reference's makePeriodic, lb.c:1783-1817) closes the
+    box: the interior mass after 40 wrapped steps equals the wrapped initial state's."""
+    import subprocess
+    lx, ly = 77, 45
+    mass = []
+    for steps in (0, 40):
+        d = tmp_path / str(steps)
+        d.mkdir()
+        subprocess.run([_PERIODIC_REF, str(lx), str(ly), str(steps), "0", str(d)], check=True,
+                       timeout=120)
+        f = np.fromfile(d / "lattice.bin", "<f8").reshape(lx + 2, ly + 2, 9)
+        mass.append(f[1:-1, 1:-1].sum())
+        assert (d / "vel.dat").read_text().count("\n") == lx * ly
+    assert abs(mass[1] - mass[0]) <= 1e-13 * mass[0], mass
