@@ -236,6 +236,10 @@ int lbgpu_batch_last_launches(lbgpu_batch *b);
 int lbgpu_batch_size_class(long long nodes);
 int lbgpu_batch_set_shape(lbgpu_batch *b, int size_class, int tile_width, int nodes_per_thread);
 int lbgpu_batch_get_shape(lbgpu_batch *b, int size_class, int *tile_width, int *nodes_per_thread);
+/* Strip length of a size class: one block steps `passes` (1..64, default 1) tiles of a member
+ * stacked in y, one after another down the lattice, and reads the member's descriptor once. */
+int lbgpu_batch_set_passes(lbgpu_batch *b, int size_class, int passes);
+int lbgpu_batch_get_passes(lbgpu_batch *b, int size_class);
 /* Launch form: 1 = a persistent grid (resident blocks per SM x SMs) strides through the work
  * list, 0 = one block per tile (the default). */
 int lbgpu_batch_set_persistent(lbgpu_batch *b, int persistent);

@@ -10,8 +10,11 @@
 // once as a CUDA graph: the kernels read each member's buffers and parities from a device
 // descriptor array, so the same graph replays chunk after chunk; it is re-captured when the
 // membership or the launch form changes.
-// Tile widths are chosen per size class of member (node count), the threads per tile and the
-// launch form per batch, by hand or by lbgpu_batch_autotune.
+// A work item is a strip of tiles of one member stacked in y: its block reads the member's
+// descriptor once and steps the tiles one after another down the lattice, so the descriptor's
+// dependent loads are spread over the strip.  Tile widths and strip lengths are chosen per size
+// class of member (node count), the threads per tile and the launch form per batch, by hand or by
+// lbgpu_batch_autotune.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -29,6 +32,7 @@ constexpr int kClasses = 6;     // node-count classes: < 16K, 64K, 256K, 1M, 4M,
 constexpr int kChunk = 50;      // steps per captured graph (even: buffer parities repeat)
 constexpr int kLists = 4;       // pull, pull four nodes a thread; AA of phase parity 0, 1 at rebuild
 constexpr int kQuad = 3;        // shape of the four-nodes-a-thread pull tiles (16-bit storage)
+constexpr int kMaxPasses = 64;  // tiles a block may step down one member
 
 int size_class(long long nodes)
 {
@@ -48,6 +52,7 @@ struct lbgpu_batch {
     cudaStream_t stream = nullptr;
     std::vector<lbgpu_lattice *> members;   // slot -> lattice (null: free slot)
     int shape[kClasses] = {2, 2, 2, 2, 2, 2};  // 0..2: 32 << shape wide; kQuad: 16-bit quad pull
+    int passes[kClasses] = {1, 1, 1, 1, 1, 1}; // tiles a block steps down the lattice
     int threads = 128;                       // nodes per tile = threads per block
     bool persistent = false;
     BatchInst *d_inst = nullptr;
@@ -173,10 +178,12 @@ int rebuild(lbgpu_batch *b)
         b->h_inst[i] = describe(L);
         int sh = b->shape[size_class((long long)L.lx * L.ly)];
         if (sh == kQuad && L.scheme == LBGPU_AA) sh = 2;   // AA steps run one node per thread
-        const int tw = tile_w(sh), th = tile_h(sh, b->threads);
+        const int np = b->passes[size_class((long long)L.lx * L.ly)];
+        const int tw = tile_w(sh), th = tile_h(sh, b->threads) * np;
         const int s = (L.scheme == LBGPU_AA) ? 2 + b->h_inst[i].phase0 : (sh == kQuad ? 1 : 0);
         for (int y0 = 1; y0 <= L.ly; y0 += th)
-            for (int x0 = 1; x0 <= L.lx; x0 += tw) work[s].push_back(BatchWork{(int)i, x0, y0, sh});
+            for (int x0 = 1; x0 <= L.lx; x0 += tw)
+                work[s].push_back(BatchWork{(int)i, x0, y0, lbgpu::batch_sp(sh, np)});
     }
     b->aa_phase = 0;
     b->rs = false;
@@ -382,6 +389,23 @@ int lbgpu_batch_get_shape(lbgpu_batch *b, int size_class_, int *tile_width, int 
     return LB_OK;
 }
 
+int lbgpu_batch_set_passes(lbgpu_batch *b, int size_class_, int passes)
+{
+    if (!b || size_class_ < 0 || size_class_ >= kClasses || passes < 1 || passes > kMaxPasses)
+        return set_error(LB_ERR_ARG, "lbgpu_batch_set_passes: size class %d, passes %d (1..%d)",
+                         size_class_, passes, kMaxPasses);
+    if (b->passes[size_class_] != passes) {
+        b->passes[size_class_] = passes;
+        b->dirty = true;
+    }
+    return LB_OK;
+}
+
+int lbgpu_batch_get_passes(lbgpu_batch *b, int size_class_)
+{
+    return (b && size_class_ >= 0 && size_class_ < kClasses) ? b->passes[size_class_] : 0;
+}
+
 int lbgpu_batch_set_persistent(lbgpu_batch *b, int persistent)
 {
     if (!b) return set_error(LB_ERR_ARG, "lbgpu_batch_set_persistent: null batch");
@@ -547,6 +571,20 @@ int lbgpu_batch_autotune(lbgpu_batch *b, int steps, float *best_ms_out)
             if (ms < best) { best = ms; best_shape = ws; }
         }
         b->shape[c] = best_shape;
+        b->dirty = true;
+        // then the strip length: how many tiles of the class one block steps
+        int best_np = b->passes[c];
+        for (int np = 1; np <= 16; np *= 2) {
+            if (np == best_np) continue;
+            const int keep = b->passes[c];
+            b->passes[c] = np;
+            b->dirty = true;
+            float ms = 0.f;
+            if (int rc = time_setting(b, steps, &ms)) return rc;
+            if (ms < best) { best = ms; best_np = np; }
+            b->passes[c] = keep;
+        }
+        b->passes[c] = best_np;
         b->dirty = true;
         if (best_ms_out) best_ms_out[c] = best;
     }

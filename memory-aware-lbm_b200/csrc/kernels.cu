@@ -1072,68 +1072,97 @@ constexpr int batch_min_blocks()
 
 // RS: the kernel also serves stochastically rounded members (16-bit only); batches without
 // any keep kernels without that code, whose registers it would otherwise raise.
+// One strip of tiles (BatchWork): the member's descriptor is read once, then the block walks its
+// passes down the lattice; every node runs the single-lattice node function.  With
+// LBGPU_BATCH_PF > 0 the rows of the tile that many passes ahead are prefetched into L2 at the
+// start of each pass (lane 0 of each warp for the warp's row segment, with prefetch_rows_l2's
+// alignment and bounds rules: tile widths and x0 - 1 are multiples of 32 nodes).
+#ifndef LBGPU_BATCH_PF
+#define LBGPU_BATCH_PF 0
+#endif
+template <class S, int NW, int ROWS>
+__device__ __forceinline__ void batch_prefetch(const Geo &g, const S *src, int x0, int Y, const uint8_t *tag)
+{
+    if constexpr (LBGPU_BATCH_PF > 0) prefetch_rows_l2<S, NW, ROWS>(g, src, x0, Y, tag);
+}
+
 template <class S, int KIND, int BT, bool RS>
-__device__ __forceinline__ void batch_node(const BatchInst *__restrict__ insts, const BatchWork it, int k)
+__device__ __forceinline__ void batch_strip(const BatchInst *__restrict__ insts, const BatchWork it, int k)
 {
     const BatchInst &d = insts[it.inst];
     const Geo g = d.g;
+    const int passes = batch_passes(it.sp);
+    S *side = static_cast<S *>(d.side) + (size_t)((d.tau0 + k) & 1) * 9 * (size_t)g.nper;
+    const double omega = d.omega;
+    const float sc = d.scale, inv = d.inv_scale;
     if constexpr (KIND == BATCH_PULL4) {
         if constexpr (sizeof(S) == 2) {
-            // warp w of the block: row y0 + w, lanes x0 + 4 lane .. x0 + 4 lane + 3
-            const int Y = it.y0 + (int)(threadIdx.x >> 5);
-            if (Y > g.ly) return;                       // uniform over the warp
+            // warp w of the block: row y0 + w of each pass, lanes x0 + 4 lane .. x0 + 4 lane + 3
             const int lane = threadIdx.x & 31;
-            S *side = static_cast<S *>(d.side) + (size_t)((d.tau0 + k) & 1) * 9 * (size_t)g.nper;
             const int src = d.cur0 ^ (k & 1);
             const S *sb = static_cast<const S *>(d.buf[src]);
             S *db = static_cast<S *>(d.buf[src ^ 1]);
             const int x0 = it.x0 + 4 * lane;
-            if (RS && d.rs) {
-                const unsigned key = rs_key(d.rs_seed, (unsigned long long)(d.tau0 + k));
-                if (g.shift_u)
-                    pull_quad<S, true, true>(g, sb, db, d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, x0, Y, lane, key);
-                else
-                    pull_quad<S, false, true>(g, sb, db, d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, x0, Y, lane, key);
-            } else if (g.shift_u) {
-                pull_quad<S, true>(g, sb, db, d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, x0, Y, lane);
-            } else {
-                pull_quad<S, false>(g, sb, db, d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, x0, Y, lane);
+            int Y = it.y0 + (int)(threadIdx.x >> 5);
+            const bool rs = RS && d.rs;
+            const unsigned key = rs ? rs_key(d.rs_seed, (unsigned long long)(d.tau0 + k)) : 0u;
+            for (int p = 0; p < passes && Y <= g.ly; ++p, Y += BT / 32) {   // uniform over the warp
+                if (LBGPU_BATCH_PF > 0 && lane == 0 && p + LBGPU_BATCH_PF < passes)
+                    batch_prefetch<S, 128, 0>(g, sb, it.x0, Y + LBGPU_BATCH_PF * (BT / 32), d.tag);
+                if (RS && rs) {
+                    if (g.shift_u) pull_quad<S, true, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane, key);
+                    else pull_quad<S, false, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane, key);
+                } else if (g.shift_u) {
+                    pull_quad<S, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane);
+                } else {
+                    pull_quad<S, false>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane);
+                }
             }
         }
         return;
     }
-    const int lw = 5 + it.shape;                       // log2 of the tile width
+    const int lw = 5 + batch_shape(it.sp);             // log2 of the tile width
     const int X = it.x0 + (int)(threadIdx.x & ((1u << lw) - 1));
-    const int Y = it.y0 + (int)(threadIdx.x >> lw);
-    if (X > g.lx || Y > g.ly) return;
-    S *side = static_cast<S *>(d.side) + (size_t)((d.tau0 + k) & 1) * 9 * (size_t)g.nper;
+    if (X > g.lx) return;
+    const int rows = BT >> lw;
+    int Y = it.y0 + (int)(threadIdx.x >> lw);
     if constexpr (RS && sizeof(S) == 2) {
         if (d.rs) {   // the single-lattice arithmetic with the member's collision key
             const unsigned key = rs_key(d.rs_seed, (unsigned long long)(d.tau0 + k));
-            if (KIND == BATCH_PULL) {
-                const int src = d.cur0 ^ (k & 1);
-                pull_node<S, 2, true>(g, static_cast<const S *>(d.buf[src]), static_cast<S *>(d.buf[src ^ 1]),
-                                      d.tag, d.bc, d.omega, side, d.scale, d.inv_scale, X, Y, key);
-            } else if (KIND == BATCH_AA_EVEN) {
-                aa_even_node<S, 2, true>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, d.omega, side, d.scale,
-                                         d.inv_scale, X, Y, key);
-            } else {
-                aa_odd_node<S, 2, true>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, d.omega, side, d.scale,
-                                        d.inv_scale, X, Y, key);
+            for (int p = 0; p < passes && Y <= g.ly; ++p, Y += rows) {
+                if (KIND == BATCH_PULL) {
+                    const int src = d.cur0 ^ (k & 1);
+                    pull_node<S, 2, true>(g, static_cast<const S *>(d.buf[src]), static_cast<S *>(d.buf[src ^ 1]),
+                                          d.tag, d.bc, omega, side, sc, inv, X, Y, key);
+                } else if (KIND == BATCH_AA_EVEN) {
+                    aa_even_node<S, 2, true>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, omega, side, sc, inv, X, Y, key);
+                } else {
+                    aa_odd_node<S, 2, true>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, omega, side, sc, inv, X, Y, key);
+                }
             }
             return;
         }
     }
-    if (KIND == BATCH_PULL) {
-        const int src = d.cur0 ^ (k & 1);
-        pull_node<S>(g, static_cast<const S *>(d.buf[src]), static_cast<S *>(d.buf[src ^ 1]), d.tag,
-                     d.bc, d.omega, side, d.scale, d.inv_scale, X, Y);
-    } else if (KIND == BATCH_AA_EVEN) {
-        aa_even_node<S>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, d.omega, side, d.scale,
-                        d.inv_scale, X, Y);
-    } else {
-        aa_odd_node<S>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, d.omega, side, d.scale,
-                       d.inv_scale, X, Y);
+    const bool pf_lane = LBGPU_BATCH_PF > 0 && (threadIdx.x & 31) == 0;   // a warp's 32 nodes
+    for (int p = 0; p < passes && Y <= g.ly; ++p, Y += rows) {
+        if (LBGPU_BATCH_PF > 0 && pf_lane && p + LBGPU_BATCH_PF < passes) {
+            const int Yp = Y + LBGPU_BATCH_PF * rows;
+            if (KIND == BATCH_PULL)
+                batch_prefetch<S, 32, 0>(g, static_cast<const S *>(d.buf[d.cur0 ^ (k & 1)]), X, Yp, nullptr);
+            else if (KIND == BATCH_AA_EVEN)
+                batch_prefetch<S, 32, 1>(g, static_cast<const S *>(d.buf[0]), X, Yp, nullptr);
+            else
+                batch_prefetch<S, 32, 2>(g, static_cast<const S *>(d.buf[0]), X, Yp, nullptr);
+        }
+        if (KIND == BATCH_PULL) {
+            const int src = d.cur0 ^ (k & 1);
+            pull_node<S>(g, static_cast<const S *>(d.buf[src]), static_cast<S *>(d.buf[src ^ 1]), d.tag,
+                         d.bc, omega, side, sc, inv, X, Y);
+        } else if (KIND == BATCH_AA_EVEN) {
+            aa_even_node<S>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, omega, side, sc, inv, X, Y);
+        } else {
+            aa_odd_node<S>(g, static_cast<S *>(d.buf[0]), d.tag, d.bc, omega, side, sc, inv, X, Y);
+        }
     }
 }
 
@@ -1142,9 +1171,9 @@ __global__ void __launch_bounds__(BT, (batch_min_blocks<S, KIND, PERSIST, BT>())
     k_batch(const BatchInst *__restrict__ insts, const BatchWork *__restrict__ work, int nwork, int k)
 {
     if (PERSIST) {
-        for (int w = blockIdx.x; w < nwork; w += gridDim.x) batch_node<S, KIND, BT, RS>(insts, work[w], k);
+        for (int w = blockIdx.x; w < nwork; w += gridDim.x) batch_strip<S, KIND, BT, RS>(insts, work[w], k);
     } else if ((int)blockIdx.x < nwork) {
-        batch_node<S, KIND, BT, RS>(insts, work[blockIdx.x], k);
+        batch_strip<S, KIND, BT, RS>(insts, work[blockIdx.x], k);
     }
 }
 

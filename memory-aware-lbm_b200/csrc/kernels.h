@@ -88,11 +88,16 @@ struct BatchInst {
     int rs;
 };
 
-// A tile of a lattice: nodes x0 .. x0 + (32 << shape) - 1 and y0 .. y0 + threads / (32 << shape) - 1
-// (BATCH_PULL4: x0 .. x0 + 127 and y0 .. y0 + threads / 32 - 1).
+// A strip of `passes` tiles of a lattice stacked in y, stepped by one block from the top down.
+// A tile: nodes x0 .. x0 + (32 << shape) - 1 and threads / (32 << shape) rows (BATCH_PULL4:
+// x0 .. x0 + 127 and threads / 32 rows); pass p covers the tile starting at row
+// y0 + p * (rows of a tile).  `sp` packs shape (bits 0..7) and passes (bits 8..).
 struct BatchWork {
-    int inst, x0, y0, shape;
+    int inst, x0, y0, sp;
 };
+__host__ __device__ inline int batch_shape(int sp) { return sp & 0xff; }
+__host__ __device__ inline int batch_passes(int sp) { return sp >> 8; }
+__host__ __device__ inline int batch_sp(int shape, int passes) { return shape | (passes << 8); }
 
 // Step k of a chunk, of kind BATCH_PULL / AA_EVEN / AA_ODD / PULL4 (16-bit only), for every tile of a
 // work list of `nwork` tiles of `threads` nodes: `persistent` grids of `grid` blocks stride

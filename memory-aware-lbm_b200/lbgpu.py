@@ -113,6 +113,8 @@ def lib():
     L.lbgpu_batch_set_shape.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.lbgpu_batch_get_shape.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_int)]
+    L.lbgpu_batch_set_passes.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
+    L.lbgpu_batch_get_passes.argtypes = [_vp, ctypes.c_int]
     L.lbgpu_batch_set_persistent.argtypes = [_vp, ctypes.c_int]
     L.lbgpu_batch_get_persistent.argtypes = [_vp]
     L.lbgpu_batch_set_threads.argtypes = [_vp, ctypes.c_int]
@@ -479,6 +481,13 @@ class Batch:
         w, n = ctypes.c_int(), ctypes.c_int()
         _check(lib().lbgpu_batch_get_shape(self.h, size_class, ctypes.byref(w), ctypes.byref(n)))
         return w.value, n.value
+
+    def set_passes(self, size_class, passes):
+        """Tiles of a size class one block steps down a member (the strip length)."""
+        _check(lib().lbgpu_batch_set_passes(self.h, int(size_class), int(passes)))
+
+    def passes(self, size_class):
+        return lib().lbgpu_batch_get_passes(self.h, int(size_class))
 
     @property
     def persistent(self):
