@@ -766,6 +766,151 @@ __global__ void __launch_bounds__(W + 2) k_sweep2(Geo g, const S *__restrict__ s
     asm volatile("cp.async.wait_group 0;" ::: "memory");   // the last prefetch lands before the block ends
 }
 
+// ---- two steps per sweep, register form ---------------------------------------------------
+//
+// The same two steps as k_sweep2 (same node arithmetic, same stale-slot and scratch handling,
+// finished by k_pull2_finish), with both steps kept in registers: each warp owns a strip of
+// SW2_OUT = 28 columns and a segment of H rows and walks down it.  Lane l holds column
+// X = x0 - 2 + l (x0 - 2 .. x0 + 29); one iteration loads row R of C_n (nine populations of the
+// lane's column), shifts directions with c_ix = +-1 one lane across by shuffles, computes step
+// n+1 on row R - 1 (lanes 1..30 are valid) and step n+2 on row R - 2 (lanes 2..29, written).  A
+// population's row shift c_iy is the walk itself: directions with c_iy = +1 come from the row
+// two iterations back, c_iy = 0 from the previous one, c_iy = -1 from the current one, so each
+// step holds nine values of the rows behind it.  No shared memory and no block barrier: warps
+// are independent, the halo (two columns a side, shared with the neighbouring strips, and two
+// rows a segment end) is re-read from L2.
+constexpr int SW2_OUT = 28;   // output columns a warp
+
+// Direction groups of the walk (D2Q9 order of lb.c:48-55): c_iy = +1 {2, 5, 6}, 0 {0, 1, 3},
+// -1 {4, 7, 8}.
+template <class W>
+__device__ __forceinline__ W lane_shift(W v, int i)
+{
+    if (cx(i) == 1) return __shfl_up_sync(0xffffffffu, v, 1);     // from lane - 1
+    if (cx(i) == -1) return __shfl_down_sync(0xffffffffu, v, 1);  // from lane + 1
+    return v;
+}
+
+// One pull step of the walk on row Y at column X of this lane: the gathered populations from the
+// held rows (up: c_iy = +1, mid: c_iy = 0) and the current one (cur, already lane-shifted),
+// stale slots from `side` on the perimeter; collides into f.
+template <class S>
+__device__ __forceinline__ void walk_gather(const Geo &g, const typename Work<S>::W up[3],
+                                            const typename Work<S>::W mid[3],
+                                            const typename Work<S>::W cur[9], const S *__restrict__ side,
+                                            float inv, int X, int Y, bool edge, int p,
+                                            typename Work<S>::W f[9])
+{
+    f[2] = up[0]; f[5] = up[1]; f[6] = up[2];
+    f[0] = mid[0]; f[1] = mid[1]; f[3] = mid[2];
+    f[4] = cur[4]; f[7] = cur[7]; f[8] = cur[8];
+    if (edge) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            if (!g.interior(X - cx(i), Y - cy(i))) f[i] = Work<S>::load(side[(size_t)i * g.nper + p], i, inv);
+    }
+}
+
+template <class S>
+__device__ __forceinline__ void walk_hold(typename Work<S>::W up_next[3], typename Work<S>::W up[3],
+                                          typename Work<S>::W mid[3], const typename Work<S>::W cur[9])
+{
+    up[0] = up_next[0]; up[1] = up_next[1]; up[2] = up_next[2];
+    up_next[0] = cur[2]; up_next[1] = cur[5]; up_next[2] = cur[6];
+    mid[0] = cur[0]; mid[1] = cur[1]; mid[2] = cur[3];
+}
+
+#ifndef LBGPU_SWEEP2W_MINB64
+#define LBGPU_SWEEP2W_MINB64 4    // blocks of 4 warps a SM for FP64 (at most 128 registers)
+#endif
+#ifndef LBGPU_SWEEP2W_MINB32
+#define LBGPU_SWEEP2W_MINB32 6    // FP32 (at most 80 registers)
+#endif
+template <class S>
+constexpr int sweep2w_min_blocks()
+{
+    return sizeof(S) == 8 ? LBGPU_SWEEP2W_MINB64 : (sizeof(S) == 4 ? LBGPU_SWEEP2W_MINB32 : 5);
+}
+
+template <class S, int H, bool RS>
+__global__ void __launch_bounds__(128, sweep2w_min_blocks<S>()) k_sweep2w(Geo g, const S *__restrict__ src, S *__restrict__ dst,
+                                                 const uint8_t *__restrict__ tag, const double *__restrict__ bc,
+                                                 double omega, const S *__restrict__ side_a,
+                                                 S *__restrict__ side_tmp, S *__restrict__ side_b, float sc,
+                                                 float inv)
+{
+    using W = typename Work<S>::W;
+    const int lane = threadIdx.x & 31;
+    const int x0 = 1 + ((int)blockIdx.x * 4 + (int)(threadIdx.x >> 5)) * SW2_OUT;
+    if (x0 > g.lx) return;                                 // the whole warp
+    const int X = x0 - 2 + lane;
+    const int y0 = 1 + (int)blockIdx.y * H;
+    const int yend = min(y0 + H, g.ly + 1);                // rows y0 .. yend-1 are this warp's
+    const bool col_in = X >= 0 && X <= g.lx + 1;           // a column of the arrays
+    const bool x_int = X >= 1 && X <= g.lx;
+    const bool own_a = lane >= 2 && lane < 2 + SW2_OUT && x_int;   // owned columns (either step)
+    W a_up[3] = {}, a_upn[3] = {}, a_mid[3] = {};          // C_n rows behind the walk
+    W b_up[3] = {}, b_upn[3] = {}, b_mid[3] = {};          // C_{n+1} rows behind the walk
+    for (int R = y0 - 2; R <= yend + 1; ++R) {
+        // C_n row R, lane-shifted
+        W cur[9];
+        if (col_in && R >= 0 && R <= g.ly + 1) {
+            const long long o = g.idx(X, R);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) cur[i] = Work<S>::load(plane(src, g, i)[o], i, inv);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) cur[i] = W(0);
+        }
+#pragma unroll
+        for (int i = 0; i < 9; ++i) cur[i] = lane_shift(cur[i], i);
+        // step n+1 on row Y1 = R - 1: its C_{n+1} values in the storage type, lane-shifted
+        const int Y1 = R - 1;
+        W nxt[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) nxt[i] = W(0);
+        if (R >= y0 && x_int && Y1 >= 1 && Y1 <= g.ly) {
+            const bool edge = g.perimeter(X, Y1);
+            const int p = edge ? g.pidx(X, Y1) : 0;
+            W f[9];
+            walk_gather<S>(g, a_up, a_mid, cur, side_a, inv, X, Y1, edge, p, f);
+            collide_w<S>(bc, g, tag[g.idx(X, Y1)], X, Y1, f, omega, sc, inv);
+            const RsNode h = rs_node<S, RS>(g, g.rs_key, X, Y1);
+#pragma unroll
+            for (int i = 0; i < 9; ++i)
+                nxt[i] = Work<S>::load(put<S, RS>(stored_out<S>(g, Y1, i, f[i], sc), i, sc, h), i, inv);
+            if (edge && own_a && lane < 2 + SW2_OUT && Y1 >= y0 && Y1 < yend) {
+#pragma unroll
+                for (int i = 0; i < 9; ++i)
+                    if (!g.interior(X - cx(i), Y1 - cy(i)))
+                        side_tmp[(size_t)i * g.nper + p] = put<S, RS>(f[i], i, sc, h);
+            }
+        }
+        walk_hold<S>(a_upn, a_up, a_mid, cur);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) nxt[i] = lane_shift(nxt[i], i);
+        // step n+2 on row Y2 = R - 2, written for the owned columns
+        const int Y2 = R - 2;
+        if (R >= y0 + 2 && own_a && Y2 < yend) {
+            const bool edge = g.perimeter(X, Y2);
+            const int p = edge ? g.pidx(X, Y2) : 0;
+            W f[9];
+            walk_gather<S>(g, b_up, b_mid, nxt, side_b, inv, X, Y2, edge, p, f);
+            const long long o = g.idx(X, Y2);
+            collide_w<S>(bc, g, tag[o], X, Y2, f, omega, sc, inv);
+            const RsNode h = rs_node<S, RS>(g, g.rs_key2, X, Y2);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) plane(dst, g, i)[o] = put<S, RS>(stored_out<S>(g, Y2, i, f[i], sc), i, sc, h);
+            if (edge) {
+#pragma unroll
+                for (int i = 0; i < 9; ++i)
+                    if (!g.interior(X - cx(i), Y2 - cy(i))) side_b[(size_t)i * g.nper + p] = put<S, RS>(f[i], i, sc, h);
+            }
+        }
+        walk_hold<S>(b_upn, b_up, b_mid, nxt);
+    }
+}
+
 // After k_sweep2: the scratch stale slots into parity (n+1)&1, and the ghost rings of the two
 // buffers exchanged (one thread per perimeter node and per ghost-ring node).
 template <class S>
@@ -1609,18 +1754,56 @@ static void launch_sweep2_t(const DevLattice &d, int src, int n_par, cudaStream_
                                          d.inv_scale);
 }
 
+// The register form (k_sweep2w) of the two-step sweep for the storage types whose bit is set in
+// LBGPU_SWEEP2_REG (1 FP64, 2 FP32, 4 FP16 / BF16); the others use the shared-memory form.
+#ifndef LBGPU_SWEEP2_REG
+#define LBGPU_SWEEP2_REG 0
+#endif
+#ifndef LBGPU_SWEEP2W_H
+#define LBGPU_SWEEP2W_H 128     // rows a warp walks
+#endif
+template <class S, bool RS = false>
+static void launch_sweep2w_t(const DevLattice &d, int src, int n_par, cudaStream_t s)
+{
+    const int strips = cdiv(d.g.lx, SW2_OUT);
+    dim3 grid(cdiv(strips, 4), cdiv(d.g.ly, LBGPU_SWEEP2W_H));
+    k_sweep2w<S, LBGPU_SWEEP2W_H, RS><<<grid, 128, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc,
+                                                          d.omega, SIDE<S>(d, n_par + 1), SIDE_TMP<S>(d),
+                                                          SIDE<S>(d, n_par), d.scale, d.inv_scale);
+}
+
 void launch_pull2(const DevLattice &d, int src, int n_par, cudaStream_t s)
 {
+    constexpr bool reg64 = (LBGPU_SWEEP2_REG & 1) != 0, reg32 = (LBGPU_SWEEP2_REG & 2) != 0,
+                   reg16 = (LBGPU_SWEEP2_REG & 4) != 0;
     switch (d.precision) {
-    case LBGPU_F64: launch_sweep2_t<double, 126, 128>(d, src, n_par, s); break;
-    case LBGPU_F32: launch_sweep2_t<float, 126, 128>(d, src, n_par, s); break;
+    case LBGPU_F64:
+        if (reg64) launch_sweep2w_t<double>(d, src, n_par, s);
+        else launch_sweep2_t<double, 126, 128>(d, src, n_par, s);
+        break;
+    case LBGPU_F32:
+        if (reg32) launch_sweep2w_t<float>(d, src, n_par, s);
+        else launch_sweep2_t<float, 126, 128>(d, src, n_par, s);
+        break;
     case LBGPU_F16:
-        if (d.g.rs_key) launch_sweep2_t<__half, 126, 128, true>(d, src, n_par, s);
-        else launch_sweep2_t<__half, 126, 128>(d, src, n_par, s);
+        if (reg16) {
+            if (d.g.rs_key) launch_sweep2w_t<__half, true>(d, src, n_par, s);
+            else launch_sweep2w_t<__half>(d, src, n_par, s);
+        } else if (d.g.rs_key) {
+            launch_sweep2_t<__half, 126, 128, true>(d, src, n_par, s);
+        } else {
+            launch_sweep2_t<__half, 126, 128>(d, src, n_par, s);
+        }
         break;
     default:
-        if (d.g.rs_key) launch_sweep2_t<__nv_bfloat16, 126, 128, true>(d, src, n_par, s);
-        else launch_sweep2_t<__nv_bfloat16, 126, 128>(d, src, n_par, s);
+        if (reg16) {
+            if (d.g.rs_key) launch_sweep2w_t<__nv_bfloat16, true>(d, src, n_par, s);
+            else launch_sweep2w_t<__nv_bfloat16>(d, src, n_par, s);
+        } else if (d.g.rs_key) {
+            launch_sweep2_t<__nv_bfloat16, 126, 128, true>(d, src, n_par, s);
+        } else {
+            launch_sweep2_t<__nv_bfloat16, 126, 128>(d, src, n_par, s);
+        }
         break;
     }
     const int nthreads = std::max(d.g.nper, d.g.nghost());
