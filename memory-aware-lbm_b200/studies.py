@@ -136,10 +136,23 @@ def batching_study(precisions=("f32", "f16"), n=512, steps=2000, seed=20260101, 
 # ------------------------------------------------------------------------------------------
 # serving
 # ------------------------------------------------------------------------------------------
+OMEGA_MAX = 1.9      # serving: uMax per request keeps omega = 1/(3 nu + 1/2) at or below this
+UMAX_RANGE = (0.02, 0.1)
+
+
+def serving_umax(re, r, omega_max=OMEGA_MAX, lo=UMAX_RANGE[0], hi=UMAX_RANGE[1]):
+    """Peak inflow velocity of a request: 0.02, raised where the channel's viscosity
+    nu = uMax 2r / Re would put omega above omega_max (small grids at high Re), capped at 0.1
+    (Mach 0.17).  Requests that need more than the cap are under-resolved on their grid."""
+    nu_min = (1.0 / omega_max - 0.5) / 3.0
+    return float(min(hi, max(lo, nu_min * re / (2.0 * r))))
+
+
 def serving_requests(n, seed=20260102, nmin=1e4, nmax=2e7, max_steps=5000, tol=1e-7,
-                     umax=0.02):
+                     umax=None):
     """Node counts log-uniform on [nmin, nmax], aspect nx/ny ~ U[2, 8], Re ~ U[20, 500];
-    obstacle at (nx/5 + 1, ny/2 + 1), radius ny/10 + 1; arrival times are set later."""
+    obstacle at (nx/5 + 1, ny/2 + 1), radius ny/10 + 1; uMax per request (serving_umax) unless
+    given; arrival times are set later."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(n):
@@ -148,64 +161,84 @@ def serving_requests(n, seed=20260102, nmin=1e4, nmax=2e7, max_steps=5000, tol=1
         ny = max(16, int(round(math.sqrt(N / aspect))))
         nx = max(32, int(round(N / ny)))
         r = ny // 10 + 1
+        re = float(rng.uniform(20, 500))
         out.append(dict(lx=nx, ly=ny, obst_x=nx // 5 + 1, obst_y=ny // 2 + 1, obst_r=r,
-                        umax=umax, re=float(rng.uniform(20, 500)), max_steps=max_steps,
-                        tol=tol, arrival=0.0, want_fields=False))
+                        umax=serving_umax(re, r) if umax is None else umax, re=re,
+                        max_steps=max_steps, tol=tol, arrival=0.0, want_fields=False))
     return out
 
 
-def _serve(prec, reqs, batched, budget, schemes=None, shapes=None, sample=(), shift=False, rs=False):
+def _serve(prec, reqs, batched, budget, schemes=None, shapes=None, sample=(), shift=False, rs=False,
+           solo_nodes=None):
     half = prec in lbgpu.DEFAULT_SCALE
     with lbgpu.Server(prec, budget, 100, shift=shift and half, stochastic=rs and half) as srv:
         for c, s in (schemes or {}).items():
             srv.set_scheme(c, s)
         for c, (w, npt) in (shapes or {}).items():
             srv.set_shape(c, w, npt)
+        if solo_nodes is not None:
+            srv.set_solo_nodes(solo_nodes)
         for k, q in enumerate(reqs):
             srv.submit(**dict(q, want_fields=k in sample))
         srv.run(batched)
         res = [srv.result(k, fields=k in sample) for k in range(len(reqs))]
         st = srv.stats()
     lat = [r["finish"] - r["arrival"] for r in res]
+    ok = [r for r in res if r["converged"] != -1]
+    useful = sum(r["steps"] * r["nodes"] for r in ok)
+    lat_ok = [r["finish"] - r["arrival"] for r in ok]
     return {"makespan_s": round(st["makespan_s"], 3),
             "mlups": round(st["lattice_updates"] / st["makespan_s"] / 1e6, 1),
+            "mlups_not_diverged": round(useful / st["makespan_s"] / 1e6, 1),
             "p50_latency_s": round(_pct(lat, 50), 4), "p99_latency_s": round(_pct(lat, 99), 4),
+            "p50_latency_not_diverged_s": round(_pct(lat_ok, 50), 4),
+            "p99_latency_not_diverged_s": round(_pct(lat_ok, 99), 4),
             "mean_latency_s": round(float(np.mean(lat)), 4),
             "peak_resident": st["peak_resident"], "peak_gb": round(st["peak_bytes"] / 1e9, 2),
             "converged": sum(1 for r in res if r["converged"] == 1),
             "diverged": sum(1 for r in res if r["converged"] == -1)}, res
 
 
-def serving_study(precisions=("f32", "f16"), n=120, seed=20260102, budget_gb=150.0,
-                  load=0.95, sample_every=50, shift=0, rs=0):
-    """shift=1: FP16/BF16 requests store offsets from their inflow profile (row shift); rs=1:
-    they round stochastically."""
+def serving_study(precisions=("f32", "f16"), n=5000, seed=20260102, budget_gb=150.0,
+                  load=0.95, sample_every=50, shift=0, rs=0, calib=400, plain_every=10,
+                  solo_nodes=-1):
+    """The request stream at the configuration's size.  Per storage type: the batched capacity
+    is calibrated on the first `calib` requests present at t = 0; Poisson arrivals at `load`
+    times that rate are then served batched and sequentially (plain solves one at a time, the
+    same storage), the same stream for both.  A 2 % sample (every `sample_every`-th request) is
+    re-run alone in FP64 for the velocity error; sequential FP64 plain solves of every
+    `plain_every`-th request give the FP64 plain rate.  shift=1: 16-bit requests store offsets
+    from their inflow profile; rs=1: they round stochastically.  solo_nodes >= 0 overrides the
+    server's size above which a request steps on its own (0: every request in the batch)."""
     reqs = serving_requests(n, seed)
     work = [q["lx"] * q["ly"] * q["max_steps"] for q in reqs]
     budget = int(budget_gb * 1e9)
     sample = set(range(0, n, sample_every))
-    out = {"requests": n, "seed": seed, "budget_gb": budget_gb, "offered_load": load, "row_shift": bool(shift),
-           "stochastic_rounding": bool(rs),
+    solo = None if solo_nodes < 0 else solo_nodes
+    out = {"requests": n, "seed": seed, "budget_gb": budget_gb, "offered_load": load,
+           "row_shift": bool(shift), "stochastic_rounding": bool(rs),
            "nodes_log_uniform": [1e4, 2e7], "max_steps": 5000, "tol": 1e-7,
-           "fp64_sample": sorted(sample), "precisions": {}}
+           "umax": f"0.02, raised to keep omega <= {OMEGA_MAX} (at most {UMAX_RANGE[1]})",
+           "requests_at_umax_cap": sum(1 for q in reqs if q["umax"] >= UMAX_RANGE[1]),
+           "total_nodes": int(sum(q["lx"] * q["ly"] for q in reqs)),
+           "fp64_sample": len(sample), "precisions": {}}
     rng = np.random.default_rng(seed + 1)
-    # FP64 re-runs of the sample (alone, same step counts) are made after the served runs
+    mean_work = float(np.mean(work))
     for prec in precisions:
         schemes = {c: v["scheme"] for c, v in
                    tune_schemes(prec, [(q["lx"], q["ly"]) for q in reqs]).items()}
-        # capacity: the batched rate on the whole request set at once (all arrive at t=0)
-        closed, _ = _serve(prec, reqs, True, budget, schemes, shift=shift, rs=rs)
-        cap = closed["mlups"] * 1e6
-        mean_work = float(np.mean(work))
-        rate = load * cap / mean_work            # requests per second
+        head = reqs[:calib]
+        closed, _ = _serve(prec, head, True, budget, schemes, shift=shift, rs=rs, solo_nodes=solo)
+        rate = load * closed["mlups"] * 1e6 / mean_work            # requests per second
         t = np.cumsum(rng.exponential(1.0 / rate, n))
         stream = [dict(q, arrival=float(t[k] - t[0])) for k, q in enumerate(reqs)]
-        served, res = _serve(prec, stream, True, budget, schemes, sample=sample, shift=shift, rs=rs)
-        # sequential plain solves: each request alone with the single-lattice pull kernel
+        served, res = _serve(prec, stream, True, budget, schemes, sample=sample, shift=shift, rs=rs,
+                             solo_nodes=solo)
         seq, _ = _serve(prec, stream, False, budget, shift=shift, rs=rs)
-        seq_closed, _ = _serve(prec, reqs, False, budget, shift=shift, rs=rs)
         errs = []
         for k in sorted(sample):
+            if res[k]["converged"] == -1:
+                continue
             q = reqs[k]
             with _channel(q, "f64", "pull") as lat:
                 lat.step(res[k]["steps"])
@@ -214,18 +247,22 @@ def serving_study(precisions=("f32", "f16"), n=120, seed=20260102, budget_gb=150
             errs.append(float(np.linalg.norm(du) / max(np.linalg.norm(np.hypot(ux, uy)), 1e-300)))
         out["precisions"][prec] = {
             "schemes": {str(k): v for k, v in schemes.items()},
-            "arrival_rate_per_s": round(rate, 3),
-            "closed_batched": closed, "closed_sequential": seq_closed,
+            "calibration_closed_batched": dict(closed, requests=calib),
+            "arrival_rate_per_s": round(rate, 4),
             "stream_batched": served, "stream_sequential": seq,
-            "throughput_ratio_closed": round(closed["mlups"] / seq_closed["mlups"], 2),
-            "velocity_rel_l2_vs_fp64": {"max": max(errs), "median": float(np.median(errs)),
-                                        "n": len(errs)}}
-    # sequential plain FP64 solves of the same requests, all present at t = 0
-    plain, _ = _serve("f64", reqs, False, budget)
-    out["closed_sequential_f64_plain"] = plain
+            "throughput_ratio_same_storage": round(served["mlups_not_diverged"] /
+                                                   max(seq["mlups_not_diverged"], 1e-9), 2),
+            "velocity_rel_l2_vs_fp64": {"max": max(errs) if errs else None,
+                                        "median": float(np.median(errs)) if errs else None,
+                                        "p90": _pct(errs, 90), "n": len(errs)}}
+    # sequential plain FP64 solves of every plain_every-th request, all present at t = 0
+    sub = reqs[::plain_every]
+    plain, _ = _serve("f64", sub, False, budget)
+    out["sequential_f64_plain"] = dict(plain, requests=len(sub))
     for prec in precisions:
         p = out["precisions"][prec]
-        p["throughput_ratio_vs_f64_plain"] = round(p["closed_batched"]["mlups"] / plain["mlups"], 2)
+        p["throughput_ratio_vs_f64_plain"] = round(p["stream_batched"]["mlups_not_diverged"] /
+                                                   max(plain["mlups_not_diverged"], 1e-9), 2)
     return out
 
 
