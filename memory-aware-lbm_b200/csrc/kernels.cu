@@ -155,19 +155,24 @@ __device__ __forceinline__ void bgk_offsets(float D[9], float omega, float sc, f
     const float q = inv * ir;
     const float ux = SHIFT ? fmaf(Jx, q, __fmul_rn(us, ir)) : Jx * q, uy = Jy * q;
     float A = fmaf(-1.5f * inv, fmaf(Jx, ux, Jy * uy), d);
-    if (SHIFT) A = fmaf(-1.5f * us, __fsub_rn(ux, us), A);
+    // shifted terms: t = ux - us; 4.5 (c.us)(c.u - c.us) is e1 = 4.5 us t for (1, 3) and
+    // e1 +- 4.5 us uy for (5, 7) and (6, 8)
+    const float t = SHIFT ? __fsub_rn(ux, us) : 0.0f;
+    if (SHIFT) A = fmaf(-1.5f * us, t, A);
     const float ux45 = (4.5f * inv) * ux, uy45 = (4.5f * inv) * uy;
     const float hs = 4.5f * us;
+    const float e1 = SHIFT ? __fmul_rn(hs, t) : 0.0f, ev = SHIFT ? __fmul_rn(hs, uy) : 0.0f;
     const float om1 = 1.0f - omega;
     const float k0 = omega * sc * (4.f / 9.f), k1 = omega * sc * (1.f / 9.f), k2 = omega * sc * (1.f / 36.f);
     D[0] = fmaf(om1, D[0], k0 * A);
     // The shifted terms use explicitly rounded operations: no multiply-add contraction may
     // differ between the kernels that inline this, so every scheme stays bit-identical.
-#define LBGPU_PAIR(I, J, K, CU45, CJ, EXTRA)                           \
+#define LBGPU_PAIR(I, J, K, CU45, CJ, EXTRA, HAS_EXTRA)                \
     {                                                                  \
         const float cj = (CJ);                                         \
         if (SHIFT) {                                                   \
-            const float a = __fmul_rn(K, __fadd_rn(fmaf(CU45, cj, A), (EXTRA))); \
+            const float a0 = fmaf(CU45, cj, A);                        \
+            const float a = __fmul_rn(K, HAS_EXTRA ? __fadd_rn(a0, (EXTRA)) : a0); \
             const float b = __fmul_rn((3.0f * inv) * K, cj);          \
             D[I] = fmaf(om1, D[I], __fadd_rn(a, b));                   \
             D[J] = fmaf(om1, D[J], __fsub_rn(a, b));                   \
@@ -178,10 +183,10 @@ __device__ __forceinline__ void bgk_offsets(float D[9], float omega, float sc, f
             D[J] = fmaf(om1, D[J], a - b);                             \
         }                                                              \
     }
-    LBGPU_PAIR(1, 3, k1, ux45, Jx, __fmul_rn(hs, __fsub_rn(ux, us)))
-    LBGPU_PAIR(2, 4, k1, uy45, Jy, 0.0f)
-    LBGPU_PAIR(5, 7, k2, __fadd_rn(ux45, uy45), __fadd_rn(Jx, Jy), __fmul_rn(hs, __fsub_rn(__fadd_rn(ux, uy), us)))
-    LBGPU_PAIR(6, 8, k2, __fsub_rn(uy45, ux45), __fsub_rn(Jy, Jx), __fmul_rn(-hs, __fadd_rn(__fsub_rn(uy, ux), us)))
+    LBGPU_PAIR(1, 3, k1, ux45, Jx, e1, true)
+    LBGPU_PAIR(2, 4, k1, uy45, Jy, 0.0f, false)
+    LBGPU_PAIR(5, 7, k2, __fadd_rn(ux45, uy45), __fadd_rn(Jx, Jy), __fadd_rn(e1, ev), true)
+    LBGPU_PAIR(6, 8, k2, __fsub_rn(uy45, ux45), __fsub_rn(Jy, Jx), __fsub_rn(e1, ev), true)
 #undef LBGPU_PAIR
 }
 
@@ -529,15 +534,21 @@ __device__ __forceinline__ uint2 pack_quad(const float D[4][9], int i, unsigned 
 }
 
 // Pull step for 16-bit storage, four nodes per thread (X = x0..x0+3 with x0 = 1 mod 4, so a
-// quad is one aligned 8-byte word pair).  Interior warps: per direction one aligned 8-byte load;
-// an x-shifted quad is assembled by byte permutes from that word pair and the neighbouring
-// 4-byte word, loaded by every lane (the adjacent lane's data, so an L1 hit).  Warps touching
-// the perimeter or the row's end run the per-node path.  The kernel is bounded by instruction
-// issue, so the collision is written for few instructions (bgk_offsets) and the boundary rules
-// stay out of line.
+// quad is one aligned 8-byte word pair).  Per direction one aligned 8-byte load; an x-shifted
+// quad is assembled by byte permutes from that word pair and the neighbouring 4-byte word,
+// loaded by every lane (the adjacent lane's data, so an L1 hit).  The kernel is bounded by
+// instruction issue, so the collision is written for few instructions (bgk_offsets) and the
+// boundary rules stay out of line.
 //
-// pull_quad runs the four nodes x0..x0+3 of row Y for one lane of a warp whose lanes cover 128
-// consecutive nodes (the choice between the vector and the per-node path is made per warp).
+// pull_quad runs the four nodes x0..x0+3 of row Y for one lane.  Rows 1 and ly run the per-node
+// path.  On every other row each lane runs the vector path; a quad whose nodes are all inside
+// 2..lx-1 stores its word pairs, a quad at either end of the row (a row's first quad holds the
+// perimeter column 1, its last the column lx and possibly nodes past the row) stores its inner
+// nodes one by one and recomputes its perimeter node with the per-node path.  So only the one
+// or two edge lanes of a row do extra work, instead of whole edge warps running per node.  The
+// vector loads of an edge quad stay inside the allocation: left of column 1 they reach the row
+// padding and ghost column (x0 - 2 >= -1), past lx they reach at most five elements into the
+// row padding or the next row, which exists because Y <= ly - 1.
 template <class S, bool SHIFT, bool RS = false>
 __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ src, S *__restrict__ dst,
                                           const uint8_t *__restrict__ tag, const double *__restrict__ bc,
@@ -545,13 +556,13 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
                                           int Y, int lane, unsigned key = 0u)
 {
     using H = Half2Ops<S>;
-    const int xw0 = x0 - 4 * lane;
-    const bool vec = (xw0 >= 2) && (xw0 + 127 <= g.lx - 1) && (Y >= 2) && (Y <= g.ly - 1);
-    if (!vec) {
+    (void)lane;
+    if (Y < 2 || Y > g.ly - 1) {
         for (int k = 0; k < 4; ++k)
             if (x0 + k <= g.lx) pull_node<S, SHIFT ? 1 : 0, RS>(g, src, dst, tag, bc, omega, side, sc, inv, x0 + k, Y, key);
         return;
     }
+    if (x0 > g.lx) return;
     const long long o = g.idx(x0, Y);
     uint2 v[9];
     unsigned e[9];
@@ -590,21 +601,34 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
             collide_w<S, SHIFT ? 1 : 0>(bc, g, (int)((tq >> (8 * k)) & 0xff), x0 + k, Y, D[k], omega, sc, inv);
     }
     const unsigned hq = quad_hash<S, RS>(g, key, x0, Y);
+    if (SHIFT) {
 #pragma unroll
-    for (int i = 0; i < 9; ++i) {
-        if (SHIFT) {
+        for (int i = 0; i < 9; ++i)
 #pragma unroll
             for (int k = 0; k < 4; ++k) D[k][i] = stored_out<S, 1>(g, Y, i, D[k][i], sc);
+    }
+    if (x0 >= 2 && x0 + 3 <= g.lx - 1) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            *reinterpret_cast<uint2 *>(plane(dst, g, i) + o) = pack_quad<S, RS>(D, i, hq);
+    } else {                         // a row's first or last quad: its inner nodes one by one
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (x0 + k < 2 || x0 + k > g.lx - 1) continue;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) plane(dst, g, i)[o + k] = put<S, RS>(D[k][i], i, sc, RsNode{hq, k});
         }
-        *reinterpret_cast<uint2 *>(plane(dst, g, i) + o) = pack_quad<S, RS>(D, i, hq);
+        if (x0 == 1) pull_node<S, SHIFT ? 1 : 0, RS>(g, src, dst, tag, bc, omega, side, sc, inv, 1, Y, key);
+        if (g.lx >= x0 && g.lx <= x0 + 3 && g.lx >= 2)
+            pull_node<S, SHIFT ? 1 : 0, RS>(g, src, dst, tag, bc, omega, side, sc, inv, g.lx, Y, key);
     }
 }
 
-// Eight blocks of 128 threads a SM (64 registers): more loads in flight than the 72-register
-// allocation's seven, for a few bytes of spills on the per-node fallback path.  The shifted form
-// holds the row's rebase values as well and keeps seven (72 registers).
+#ifndef LBGPU_PULL4H_SHIFT_MINB
+#define LBGPU_PULL4H_SHIFT_MINB 7   // resident blocks of the row-shifted form (72 registers)
+#endif
 template <class S, bool SHIFT, bool RS>
-__global__ void __launch_bounds__(BX, SHIFT ? 7 : 8) k_pull4h(Geo g, const S *__restrict__ src, S *__restrict__ dst,
+__global__ void __launch_bounds__(BX, SHIFT ? LBGPU_PULL4H_SHIFT_MINB : 8) k_pull4h(Geo g, const S *__restrict__ src, S *__restrict__ dst,
                                                const uint8_t *__restrict__ tag,
                                                const double *__restrict__ bc, double omega,
                                                S *__restrict__ side, float sc, float inv)
@@ -1109,8 +1133,11 @@ __global__ void __launch_bounds__(BX, SHIFT ? 7 : 8) k_aa4_even(Geo g, S *__rest
     for (int i = 0; i < 9; ++i) *reinterpret_cast<uint2 *>(plane(a, g, opp(i)) + o) = pack_quad<S, RS>(D, i, hq);
 }
 
+#ifndef LBGPU_AA4_ODD_MINB
+#define LBGPU_AA4_ODD_MINB 7        // resident blocks of the odd AA step (72 registers)
+#endif
 template <class S, bool SHIFT, bool RS>
-__global__ void __launch_bounds__(BX, SHIFT ? 6 : 7) k_aa4_odd(Geo g, S *__restrict__ a, const uint8_t *__restrict__ tag,
+__global__ void __launch_bounds__(BX, SHIFT ? LBGPU_AA4_ODD_MINB - 1 : LBGPU_AA4_ODD_MINB) k_aa4_odd(Geo g, S *__restrict__ a, const uint8_t *__restrict__ tag,
                                                  const double *__restrict__ bc, double omega,
                                                  S *__restrict__ side, float sc, float inv)
 {

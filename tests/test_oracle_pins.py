@@ -124,3 +124,4 @@ def test_reference_periodic_driver_conserves_mass(tmp_path):
         mass.append(f[1:-1, 1:-1].sum())
         assert (d / "vel.dat").read_text().count("\n") == lx * ly
     assert abs(mass[1] - mass[0]) <= 1e-13 * mass[0], mass
+
