@@ -44,7 +44,7 @@ sys.path.insert(0, PKG)
 # 16-bit suffixes (lbgpu.storage_form): "s" offsets from the inflow profile per row, "r"
 # stochastic rounding; neither changes the bytes moved
 BYTES_PER_UPDATE = {"f64": 144, "f32": 72, **{p + sfx: 36 for p in ("f16", "bf16")
-                                              for sfx in ("", "s", "r", "sr")}}
+                                              for sfx in ("", "s", "b", "r", "sr", "br")}}
 
 
 def parse():

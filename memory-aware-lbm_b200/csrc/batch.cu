@@ -69,6 +69,7 @@ struct lbgpu_batch {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};   // one chunk, by aa_phase
     int launches = 0;
     bool rs = false;                         // some member rounds stochastically (set at rebuild)
+    bool shift = false;                      // some member stores row-shifted offsets (set at rebuild)
 };
 
 namespace {
@@ -187,7 +188,11 @@ int rebuild(lbgpu_batch *b)
     }
     b->aa_phase = 0;
     b->rs = false;
-    for (const BatchInst &d : b->h_inst) b->rs = b->rs || d.rs;
+    b->shift = false;
+    for (const BatchInst &d : b->h_inst) {
+        b->rs = b->rs || d.rs;
+        b->shift = b->shift || d.g.shift_u != nullptr;
+    }
     int need[kLists];
     for (int s = 0; s < kLists; ++s) need[s] = (int)work[s].size();
     if (int rc = ensure_capacity(b, (int)std::max<size_t>(b->h_inst.size(), 1), need)) return rc;
@@ -229,7 +234,8 @@ void launch_step(lbgpu_batch *b, int k)
         }
         const int t = b->threads == 512 ? 2 : (b->threads == 256 ? 1 : 0);
         const int grid = b->persistent ? std::min(b->per_sm[kind][t] * b->sms, b->nwork[s]) : b->nwork[s];
-        lbgpu::launch_batch(b->precision, kind, b->threads, b->persistent, b->rs, b->d_inst, b->d_work[s],
+        lbgpu::launch_batch(b->precision, kind, b->threads, b->persistent, (b->rs ? 1 : 0) | (b->shift ? 2 : 0),
+                            b->d_inst, b->d_work[s],
                             b->nwork[s], grid, k, b->stream);
         ++b->launches;
     }
@@ -458,10 +464,12 @@ int lbgpu_batch_step(lbgpu_batch *b, int nsteps)
         --nsteps;
         b->dirty = true;
     }
-    // rounding switched (or reseeded) on a member since the descriptors were written
+    // rounding switched (or reseeded), or a row shift set or cleared, on a member since the
+    // descriptors were written
     for (size_t i = 0; i < b->members.size() && !b->dirty; ++i)
         if (b->members[i] && (i >= b->h_inst.size() || b->h_inst[i].rs != (b->members[i]->L.rs ? 1 : 0) ||
-                              b->h_inst[i].rs_seed != b->members[i]->L.rs_seed))
+                              b->h_inst[i].rs_seed != b->members[i]->L.rs_seed ||
+                              b->h_inst[i].g.shift_u != b->members[i]->L.d.g.shift_u))
             b->dirty = true;
     if (b->dirty)
         if (int rc = rebuild(b)) return rc;

@@ -259,12 +259,13 @@ __device__ __forceinline__ S enc_row(const Geo &g, typename Codec<S>::R f, int i
 // shift it is relative to the row that consumes it after streaming, Y + c_iy (stale-slot copies
 // in the side store are consumed by the node itself and stay relative to row Y).
 // SH: 0 no shift, 1 shift (known at compile time), 2 decided by g.shift_u at run time.
+// Rows whose rebase values are all zero (shift_rebased false) store unchanged in every kernel.
 template <class S, int SH = 2>
 __device__ __forceinline__ typename Work<S>::W stored_out(const Geo &g, int Y, int i, typename Work<S>::W w,
                                                           float sc)
 {
     if constexpr (sizeof(S) == 2 && SH != 0) {
-        if (cy(i) != 0 && (SH == 1 || g.shift_u))
+        if (cy(i) != 0 && (SH == 1 || g.shift_u) && g.shift_rebased(Y))
             return __fadd_rn(w, __fmul_rn(g.shift_rebase(Y)[i], sc));
     }
     return w;
@@ -601,7 +602,7 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
             collide_w<S, SHIFT ? 1 : 0>(bc, g, (int)((tq >> (8 * k)) & 0xff), x0 + k, Y, D[k], omega, sc, inv);
     }
     const unsigned hq = quad_hash<S, RS>(g, key, x0, Y);
-    if (SHIFT) {
+    if (SHIFT && g.shift_rebased(Y)) {
 #pragma unroll
         for (int i = 0; i < 9; ++i)
 #pragma unroll
@@ -844,6 +845,9 @@ __device__ __forceinline__ void walk_hold(typename Work<S>::W up_next[3], typena
     mid[0] = cur[0]; mid[1] = cur[1]; mid[2] = cur[3];
 }
 
+#ifndef LBGPU_SWEEP2W_PF
+#define LBGPU_SWEEP2W_PF 0         // rows ahead of the walk prefetched into L2 (0: none)
+#endif
 #ifndef LBGPU_SWEEP2W_MINB64
 #define LBGPU_SWEEP2W_MINB64 4    // blocks of 4 warps a SM for FP64 (at most 128 registers)
 #endif
@@ -875,16 +879,39 @@ __global__ void __launch_bounds__(128, sweep2w_min_blocks<S>()) k_sweep2w(Geo g,
     const bool own_a = lane >= 2 && lane < 2 + SW2_OUT && x_int;   // owned columns (either step)
     W a_up[3] = {}, a_upn[3] = {}, a_mid[3] = {};          // C_n rows behind the walk
     W b_up[3] = {}, b_upn[3] = {}, b_mid[3] = {};          // C_{n+1} rows behind the walk
-    for (int R = y0 - 2; R <= yend + 1; ++R) {
-        // C_n row R, lane-shifted
-        W cur[9];
+    // Row R + 1 is loaded while row R is computed (its values are first used one iteration
+    // later), and with LBGPU_SWEEP2W_PF > 0 lane 0 prefetches into L2 the strip's row that many
+    // rows ahead: 32 elements from column x0 - 2, widened to 16-byte boundaries and by 16 bytes,
+    // skipped where the segment would pass the row's pitch (every byte inside its plane).
+    S raw[9];
+    auto fetch = [&](int R) {
         if (col_in && R >= 0 && R <= g.ly + 1) {
             const long long o = g.idx(X, R);
 #pragma unroll
-            for (int i = 0; i < 9; ++i) cur[i] = Work<S>::load(plane(src, g, i)[o], i, inv);
+            for (int i = 0; i < 9; ++i) raw[i] = plane(src, g, i)[o];
         } else {
 #pragma unroll
-            for (int i = 0; i < 9; ++i) cur[i] = W(0);
+            for (int i = 0; i < 9; ++i) raw[i] = S(0);
+        }
+    };
+    fetch(y0 - 2);
+    for (int R = y0 - 2; R <= yend + 1; ++R) {
+        // C_n row R, lane-shifted
+        W cur[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) cur[i] = Work<S>::load(raw[i], i, inv);
+        fetch(R + 1);
+        if (LBGPU_SWEEP2W_PF > 0 && lane == 0) {
+            const int Rp = R + 1 + LBGPU_SWEEP2W_PF;
+            constexpr int EB = (int)sizeof(S);
+            const long long e0 = g.idx(x0 - 2, Rp);                       // element of column x0 - 2
+            const long long b0 = (e0 * EB) & ~15LL, b1 = ((e0 + 32) * EB + 31) & ~15LL;
+            if (Rp <= g.ly + 1 && b1 <= ((long long)Rp + 1) * g.pitch * EB)
+#pragma unroll
+                for (int i = 0; i < 9; ++i)
+                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
+                                     reinterpret_cast<const char *>(plane(src, g, i)) + b0),
+                                 "r"((unsigned)(b1 - b0)) : "memory");
         }
 #pragma unroll
         for (int i = 0; i < 9; ++i) cur[i] = lane_shift(cur[i], i);
@@ -1095,7 +1122,7 @@ __device__ __forceinline__ void aa_collide_quad(const Geo &g, const uint8_t *__r
         for (int k = 0; k < 4; ++k)
             collide_w<S, SHIFT ? 1 : 0>(bc, g, (int)((tq >> (8 * k)) & 0xff), x0 + k, Y, D[k], omega, sc, inv);
     }
-    if (SHIFT) {
+    if (SHIFT && g.shift_rebased(Y)) {
 #pragma unroll
         for (int i = 0; i < 9; ++i)
 #pragma unroll
@@ -1258,9 +1285,13 @@ __device__ __forceinline__ void batch_prefetch(const Geo &g, const S *src, int x
     if constexpr (LBGPU_BATCH_PF > 0) prefetch_rows_l2<S, NW, ROWS>(g, src, x0, Y, tag);
 }
 
-template <class S, int KIND, int BT, bool RS>
+// F: bit 0 -- some member rounds stochastically (RS paths compiled in); bit 1 -- some member
+// stores 16-bit offsets with a row shift (the shifted quad path compiled in).  Batches without
+// either keep kernels without that code, whose registers it would otherwise raise.
+template <class S, int KIND, int BT, int F>
 __device__ __forceinline__ void batch_strip(const BatchInst *__restrict__ insts, const BatchWork it, int k)
 {
+    constexpr bool RS = (F & 1) != 0, SHQ = (F & 2) != 0;
     const BatchInst &d = insts[it.inst];
     const Geo g = d.g;
     const int passes = batch_passes(it.sp);
@@ -1282,9 +1313,9 @@ __device__ __forceinline__ void batch_strip(const BatchInst *__restrict__ insts,
                 if (LBGPU_BATCH_PF > 0 && lane == 0 && p + LBGPU_BATCH_PF < passes)
                     batch_prefetch<S, 128, 0>(g, sb, it.x0, Y + LBGPU_BATCH_PF * (BT / 32), d.tag);
                 if (RS && rs) {
-                    if (g.shift_u) pull_quad<S, true, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane, key);
+                    if (SHQ && g.shift_u) pull_quad<S, true, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane, key);
                     else pull_quad<S, false, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane, key);
-                } else if (g.shift_u) {
+                } else if (SHQ && g.shift_u) {
                     pull_quad<S, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane);
                 } else {
                     pull_quad<S, false>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane);
@@ -1338,14 +1369,14 @@ __device__ __forceinline__ void batch_strip(const BatchInst *__restrict__ insts,
     }
 }
 
-template <class S, int KIND, bool PERSIST, int BT, bool RS = false>
+template <class S, int KIND, bool PERSIST, int BT, int F = 0>
 __global__ void __launch_bounds__(BT, (batch_min_blocks<S, KIND, PERSIST, BT>()))
     k_batch(const BatchInst *__restrict__ insts, const BatchWork *__restrict__ work, int nwork, int k)
 {
     if (PERSIST) {
-        for (int w = blockIdx.x; w < nwork; w += gridDim.x) batch_strip<S, KIND, BT, RS>(insts, work[w], k);
+        for (int w = blockIdx.x; w < nwork; w += gridDim.x) batch_strip<S, KIND, BT, F>(insts, work[w], k);
     } else if ((int)blockIdx.x < nwork) {
-        batch_strip<S, KIND, BT, RS>(insts, work[blockIdx.x], k);
+        batch_strip<S, KIND, BT, F>(insts, work[blockIdx.x], k);
     }
 }
 
@@ -1887,26 +1918,33 @@ void launch_aa_odd(const DevLattice &d, int side_par, cudaStream_t s)
                        SIDE<S>(d, side_par), d.scale, d.inv_scale)));
 }
 
-template <class S, int KIND, int BT, bool RS>
+template <class S, int KIND, int BT, int F>
 static void launch_batch_r(bool persistent, const BatchInst *insts, const BatchWork *work, int nwork, int grid,
                            int k, cudaStream_t s)
 {
-    if (persistent) k_batch<S, KIND, true, BT, RS><<<grid, BT, 0, s>>>(insts, work, nwork, k);
-    else k_batch<S, KIND, false, BT, RS><<<grid, BT, 0, s>>>(insts, work, nwork, k);
+    if (persistent) k_batch<S, KIND, true, BT, F><<<grid, BT, 0, s>>>(insts, work, nwork, k);
+    else k_batch<S, KIND, false, BT, F><<<grid, BT, 0, s>>>(insts, work, nwork, k);
 }
 
+// flags: bit 0 stochastic rounding, bit 1 row shift (kernels.h launch_batch); the shift matters
+// to the quad kind only.
 template <class S, int KIND, int BT>
-static void launch_batch_b(bool persistent, bool rs, const BatchInst *insts, const BatchWork *work, int nwork,
+static void launch_batch_b(bool persistent, int flags, const BatchInst *insts, const BatchWork *work, int nwork,
                            int grid, int k, cudaStream_t s)
 {
     if constexpr (sizeof(S) == 2) {
-        if (rs) return launch_batch_r<S, KIND, BT, true>(persistent, insts, work, nwork, grid, k, s);
+        const int f = KIND == BATCH_PULL4 ? (flags & 3) : (flags & 1);
+        if (f == 1) return launch_batch_r<S, KIND, BT, 1>(persistent, insts, work, nwork, grid, k, s);
+        if constexpr (KIND == BATCH_PULL4) {
+            if (f == 2) return launch_batch_r<S, KIND, BT, 2>(persistent, insts, work, nwork, grid, k, s);
+            if (f == 3) return launch_batch_r<S, KIND, BT, 3>(persistent, insts, work, nwork, grid, k, s);
+        }
     }
-    launch_batch_r<S, KIND, BT, false>(persistent, insts, work, nwork, grid, k, s);
+    launch_batch_r<S, KIND, BT, 0>(persistent, insts, work, nwork, grid, k, s);
 }
 
 template <class S, int KIND>
-static void launch_batch_k(int bt, bool persistent, bool rs, const BatchInst *insts, const BatchWork *work,
+static void launch_batch_k(int bt, bool persistent, int rs, const BatchInst *insts, const BatchWork *work,
                            int nwork, int grid, int k, cudaStream_t s)
 {
     if (bt == 512) launch_batch_b<S, KIND, 512>(persistent, rs, insts, work, nwork, grid, k, s);
@@ -1915,7 +1953,7 @@ static void launch_batch_k(int bt, bool persistent, bool rs, const BatchInst *in
 }
 
 template <class S>
-static void launch_batch_t(int kind, int bt, bool persistent, bool rs, const BatchInst *insts,
+static void launch_batch_t(int kind, int bt, bool persistent, int rs, const BatchInst *insts,
                            const BatchWork *work, int nwork, int grid, int k, cudaStream_t s)
 {
     if (kind == BATCH_PULL) launch_batch_k<S, BATCH_PULL>(bt, persistent, rs, insts, work, nwork, grid, k, s);
@@ -1927,12 +1965,12 @@ static void launch_batch_t(int kind, int bt, bool persistent, bool rs, const Bat
         launch_batch_k<S, BATCH_PULL4>(bt, persistent, rs, insts, work, nwork, grid, k, s);
 }
 
-void launch_batch(int precision, int kind, int threads, bool persistent, bool rs, const BatchInst *insts,
+void launch_batch(int precision, int kind, int threads, bool persistent, int rs, const BatchInst *insts,
                   const BatchWork *work, int nwork, int grid, int k, cudaStream_t s)
 {
     switch (precision) {
-    case LBGPU_F64: launch_batch_t<double>(kind, threads, persistent, false, insts, work, nwork, grid, k, s); break;
-    case LBGPU_F32: launch_batch_t<float>(kind, threads, persistent, false, insts, work, nwork, grid, k, s); break;
+    case LBGPU_F64: launch_batch_t<double>(kind, threads, persistent, 0, insts, work, nwork, grid, k, s); break;
+    case LBGPU_F32: launch_batch_t<float>(kind, threads, persistent, 0, insts, work, nwork, grid, k, s); break;
     case LBGPU_F16: launch_batch_t<__half>(kind, threads, persistent, rs, insts, work, nwork, grid, k, s); break;
     default: launch_batch_t<__nv_bfloat16>(kind, threads, persistent, rs, insts, work, nwork, grid, k, s); break;
     }

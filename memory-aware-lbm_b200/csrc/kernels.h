@@ -102,8 +102,9 @@ __host__ __device__ inline int batch_sp(int shape, int passes) { return shape | 
 // Step k of a chunk, of kind BATCH_PULL / AA_EVEN / AA_ODD / PULL4 (16-bit only), for every tile of a
 // work list of `nwork` tiles of `threads` nodes: `persistent` grids of `grid` blocks stride
 // through the list, otherwise `grid` must equal nwork (one block per tile).
-// rs: some member rounds stochastically (16-bit batches; the kernels then carry that path).
-void launch_batch(int precision, int kind, int threads, bool persistent, bool rs, const BatchInst *insts,
+// flags (16-bit batches): bit 0 -- some member rounds stochastically, bit 1 -- some member stores
+// row-shifted offsets; the kernels then carry those paths.
+void launch_batch(int precision, int kind, int threads, bool persistent, int flags, const BatchInst *insts,
                   const BatchWork *work, int nwork, int grid, int k, cudaStream_t s);
 // Resident blocks per SM of the persistent kernel of a kind and block size.
 int batch_blocks_per_sm(int precision, int kind, int threads);

@@ -28,7 +28,9 @@ struct Geo {
     // 16-bit storage only: the per-row shift table (device), or null.  Stored values are then
     // relative to S_i(Y) = f_eq_i(1, (u_s(Y), 0)) of the row that consumes them instead of to
     // w_i.  Layout, all float, Y = 0..ly+1: u_s[Y]; base[Y][9] = S_i(Y); rebase[Y][9] =
-    // S_i(Y) - S_i(Y + c_iy) (0 where c_iy = 0 or the row is a ghost row).
+    // S_i(Y) - S_i(Y + c_iy) (0 where c_iy = 0 or Y + c_iy is outside 0..ly+1); rows[Y] = 1 where
+    // some rebase[Y][i] is not zero, else 0 (a profile constant over bands of rows needs the
+    // rebase only on the rows at a band's edge).
     const float *shift_u;
     // 16-bit storage only: stochastic rounding keys (codec.cuh) of the launch's collision and,
     // for the two-step sweep, of the second one; 0 rounds to nearest.
@@ -38,6 +40,7 @@ struct Geo {
     {
         return shift_u + 10 * (ly + 2) + 9 * Y;
     }
+    __host__ __device__ __forceinline__ bool shift_rebased(int Y) const { return shift_u[19 * (ly + 2) + Y] != 0.0f; }
 
     __host__ __device__ __forceinline__ long long idx(int X, int Y) const
     {

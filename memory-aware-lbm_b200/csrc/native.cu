@@ -142,7 +142,7 @@ int lbgpu_set_offset_shift(lbgpu_lattice *h, const double *u_row)
     // the table of Geo::shift_u: u_s[Y], S_i(Y), S_i(Y) - S_i(Y + c_iy) (layout.cuh), in FP64
     // from the float velocities, then rounded once, so every kernel reads the same values
     const int ny2 = L.ly + 2;
-    std::vector<float> u(19 * (size_t)ny2, 0.0f);
+    std::vector<float> u(20 * (size_t)ny2, 0.0f);
     for (int Y = 0; Y < ny2; ++Y) {
         if (!(u_row[Y] > -0.5 && u_row[Y] < 0.5))
             return set_error(LB_ERR_ARG, "lbgpu_set_offset_shift: u[%d] = %g out of range", Y, u_row[Y]);
@@ -157,6 +157,7 @@ int lbgpu_set_offset_shift(lbgpu_lattice *h, const double *u_row)
             u[ny2 + 9 * Y + i] = (float)S(i, Y);
             const int Yc = Y + lbgpu::cy(i);
             if (lbgpu::cy(i) != 0 && Yc >= 0 && Yc < ny2) u[10 * ny2 + 9 * Y + i] = (float)(S(i, Y) - S(i, Yc));
+            if (u[10 * ny2 + 9 * Y + i] != 0.0f) u[19 * ny2 + Y] = 1.0f;
         }
     if (!L.shift) {
         void *p = nullptr;

@@ -343,26 +343,48 @@ def poiseuille_profile(ly, umax):
     return u
 
 
+SHIFT_BAND = 64
+
+
+def banded_profile(ly, umax, band=SHIFT_BAND):
+    """The inflow profile held constant over bands of `band` rows (each band takes the value of
+    its middle row; 0 in the ghost rows).  Offsets streamed between two rows of one band need no
+    rebase, so only the rows at a band's edge pay for it; with bands of 64 rows the stored
+    offsets stay nearly as small as with the exact profile."""
+    exact = poiseuille_profile(ly, umax)
+    u = exact.copy()
+    for y0 in range(1, ly + 1, band):
+        y1 = min(ly, y0 + band - 1)
+        u[y0:y1 + 1] = exact[(y0 + y1) // 2]
+    return u
+
+
 def storage_form(name):
     """Storage names: 'f64', 'f32', 'f16', 'bf16', and for the 16-bit types the suffixes 's'
-    (offsets from the channel's inflow-profile equilibrium per row, lbgpu_set_offset_shift) and
-    'r' (stochastic rounding, lbgpu_set_stochastic_rounding), e.g. 'f16sr'.
-    Returns (precision, shift, stochastic)."""
+    (offsets from the channel's inflow-profile equilibrium per row, lbgpu_set_offset_shift) or
+    'b' (the same profile held constant over bands of SHIFT_BAND rows, banded_profile), and 'r'
+    (stochastic rounding, lbgpu_set_stochastic_rounding), e.g. 'f16sr', 'f16br'.
+    Returns (precision, shift, stochastic) with shift '' (none), 's' or 'b'."""
     import re
-    m = re.fullmatch(r"(f64|f32|f16|bf16)(s?)(r?)", name)
+    m = re.fullmatch(r"(f64|f32|f16|bf16)([sb]?)(r?)", name)
     if not m or (m.group(1) in ("f64", "f32") and (m.group(2) or m.group(3))):
         raise ValueError(f"storage {name!r}")
-    return m.group(1), bool(m.group(2)), bool(m.group(3))
+    return m.group(1), m.group(2), bool(m.group(3))
+
+
+def shift_profile(kind, ly, umax):
+    """The per-row shift velocities of a storage's shift kind ('s' or 'b')."""
+    return banded_profile(ly, umax) if kind == "b" else poiseuille_profile(ly, umax)
 
 
 def configure_storage(lat, name, umax, seed=0):
-    """Offset scale, row shift (the inflow profile of peak umax) and rounding of a storage name,
-    applied before the initial state is written."""
+    """Offset scale, row shift (the inflow profile of peak umax, exact or banded) and rounding of
+    a storage name, applied before the initial state is written."""
     base, shift, rs = storage_form(name)
     if base in DEFAULT_SCALE:
         lat.set_offset_scale((DEFAULT_SHIFT_SCALE if shift else DEFAULT_SCALE)[base])
     if shift:
-        lat.set_offset_shift(poiseuille_profile(lat.ly, umax))
+        lat.set_offset_shift(shift_profile(shift, lat.ly, umax))
     if rs:
         lat.set_stochastic_rounding(True, seed)
 

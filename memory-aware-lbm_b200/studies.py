@@ -323,8 +323,10 @@ def precision_study(nx=16384, ny=4096, steps=20000, cases=((100.0, 0.02), (1000.
                           "non_finite": r["non_finite"],
                           "scale_log2": (lbgpu.DEFAULT_SHIFT_SCALE if lbgpu.storage_form(prec)[1]
                                          else lbgpu.DEFAULT_SCALE)[lbgpu.storage_form(prec)[0]],
-                          "offsets_from": "Poiseuille-profile equilibrium per row"
-                          if lbgpu.storage_form(prec)[1] else "w_i",
+                          "offsets_from": {"s": "Poiseuille-profile equilibrium per row",
+                                           "b": f"Poiseuille-profile equilibrium per band of "
+                                                f"{lbgpu.SHIFT_BAND} rows",
+                                           "": "w_i"}[lbgpu.storage_form(prec)[1]],
                           "rounding": "stochastic" if lbgpu.storage_form(prec)[2] else "nearest"}
             del r
         out["cases"].append(case)

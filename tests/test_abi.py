@@ -203,14 +203,29 @@ def test_reference_keeps_its_own_symbols_when_the_gpu_library_is_global():
 
 
 def test_storage_names():
-    """bench.py and the studies name storage forms; 's' and 'r' are 16-bit options only."""
-    assert lbgpu.storage_form("f64") == ("f64", False, False)
-    assert lbgpu.storage_form("f16s") == ("f16", True, False)
-    assert lbgpu.storage_form("bf16r") == ("bf16", False, True)
-    assert lbgpu.storage_form("f16sr") == ("f16", True, True)
-    for bad in ("f32r", "f64s", "f16rs", "fp16", ""):
+    """bench.py and the studies name storage forms; 's', 'b' and 'r' are 16-bit options only."""
+    assert lbgpu.storage_form("f64") == ("f64", "", False)
+    assert lbgpu.storage_form("f16s") == ("f16", "s", False)
+    assert lbgpu.storage_form("bf16r") == ("bf16", "", True)
+    assert lbgpu.storage_form("f16sr") == ("f16", "s", True)
+    assert lbgpu.storage_form("f16br") == ("f16", "b", True)
+    for bad in ("f32r", "f64s", "f32b", "f16rs", "f16sb", "fp16", ""):
         with pytest.raises(ValueError):
             lbgpu.storage_form(bad)
+
+
+def test_banded_shift_profile():
+    """Bands of SHIFT_BAND rows hold the inflow profile's value at their middle row; the ghost
+    rows stay at rest, and consecutive rows inside a band share one shift velocity."""
+    ly, umax = 300, 0.05
+    exact = lbgpu.poiseuille_profile(ly, umax)
+    band = lbgpu.banded_profile(ly, umax)
+    assert band[0] == 0.0 and band[ly + 1] == 0.0
+    b = lbgpu.SHIFT_BAND
+    for y0 in range(1, ly + 1, b):
+        y1 = min(ly, y0 + b - 1)
+        assert np.all(band[y0:y1 + 1] == exact[(y0 + y1) // 2])
+    assert np.max(np.abs(band - exact)) <= 4 * umax * (b / 2) / (ly - 1)
 
 
 def test_stochastic_rounding_setter_rejects_a_null_lattice():
