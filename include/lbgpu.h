@@ -236,7 +236,7 @@ int lbgpu_batch_last_launches(lbgpu_batch *b);
 int lbgpu_batch_size_class(long long nodes);
 int lbgpu_batch_set_shape(lbgpu_batch *b, int size_class, int tile_width, int nodes_per_thread);
 int lbgpu_batch_get_shape(lbgpu_batch *b, int size_class, int *tile_width, int *nodes_per_thread);
-/* Strip length of a size class: one block steps `passes` (1..64, default 1) tiles of a member
+/* Strip length of a size class: one block steps `passes` (1..64, default 4) tiles of a member
  * stacked in y, one after another down the lattice, and reads the member's descriptor once. */
 int lbgpu_batch_set_passes(lbgpu_batch *b, int size_class, int passes);
 int lbgpu_batch_get_passes(lbgpu_batch *b, int size_class);

@@ -235,16 +235,22 @@ def serving_study(precisions=("f32", "f16"), n=5000, seed=20260102, budget_gb=15
         served, res = _serve(prec, stream, True, budget, schemes, sample=sample, shift=shift, rs=rs,
                              solo_nodes=solo)
         seq, _ = _serve(prec, stream, False, budget, shift=shift, rs=rs)
-        errs = []
+        errs, detail = [], []
         for k in sorted(sample):
-            if res[k]["converged"] == -1:
-                continue
             q = reqs[k]
+            if res[k]["converged"] == -1:
+                detail.append({"id": k, "nodes": q["lx"] * q["ly"], "re": round(q["re"], 1),
+                               "umax": round(q["umax"], 4), "diverged": True})
+                continue
             with _channel(q, "f64", "pull") as lat:
                 lat.step(res[k]["steps"])
                 _, ux, uy = lat.macros()
             du = np.hypot(res[k]["ux"] - ux, res[k]["uy"] - uy)
             errs.append(float(np.linalg.norm(du) / max(np.linalg.norm(np.hypot(ux, uy)), 1e-300)))
+            detail.append({"id": k, "nodes": q["lx"] * q["ly"], "re": round(q["re"], 1),
+                           "umax": round(q["umax"], 4), "steps": res[k]["steps"], "err": errs[-1]})
+        capped = [d["err"] for d in detail if "err" in d and d["umax"] >= UMAX_RANGE[1]]
+        below = [d["err"] for d in detail if "err" in d and d["umax"] < UMAX_RANGE[1]]
         out["precisions"][prec] = {
             "schemes": {str(k): v for k, v in schemes.items()},
             "calibration_closed_batched": dict(closed, requests=calib),
@@ -254,7 +260,13 @@ def serving_study(precisions=("f32", "f16"), n=5000, seed=20260102, budget_gb=15
                                                    max(seq["mlups_not_diverged"], 1e-9), 2),
             "velocity_rel_l2_vs_fp64": {"max": max(errs) if errs else None,
                                         "median": float(np.median(errs)) if errs else None,
-                                        "p90": _pct(errs, 90), "n": len(errs)}}
+                                        "p90": _pct(errs, 90), "n": len(errs),
+                                        "below_umax_cap": {"n": len(below), "median": _pct(below, 50),
+                                                           "p90": _pct(below, 90),
+                                                           "max": max(below) if below else None},
+                                        "at_umax_cap": {"n": len(capped), "median": _pct(capped, 50),
+                                                        "max": max(capped) if capped else None},
+                                        "requests": detail}}
     # sequential plain FP64 solves of every plain_every-th request, all present at t = 0
     sub = reqs[::plain_every]
     plain, _ = _serve("f64", sub, False, budget)
