@@ -1167,6 +1167,9 @@ __global__ void __launch_bounds__(BX, SHIFT ? 7 : 8) k_aa4_even(Geo g, S *__rest
     for (int i = 0; i < 9; ++i) *reinterpret_cast<uint2 *>(plane(a, g, opp(i)) + o) = pack_quad<S, RS>(D, i, hq);
 }
 
+#ifndef LBGPU_AA4_ODD_SPLIT
+#define LBGPU_AA4_ODD_SPLIT 0       // 1: shifted word pairs stored as two 4-byte halves
+#endif
 #ifndef LBGPU_AA4_ODD_MINB
 #define LBGPU_AA4_ODD_MINB 7        // resident blocks of the odd AA step (72 registers)
 #endif
@@ -1215,6 +1218,20 @@ __global__ void __launch_bounds__(BX, SHIFT ? LBGPU_AA4_ODD_MINB - 1 : LBGPU_AA4
         unsigned short *h = reinterpret_cast<unsigned short *>(drow);
         if (cx(i) == 0) {
             *reinterpret_cast<uint2 *>(drow) = make_uint2(w0, w1);
+        } else if (LBGPU_AA4_ODD_SPLIT && cx(i) == 1) {   // as below, every branch a single store
+            const unsigned pw = __shfl_up_sync(0xffffffffu, w1, 1);
+            const unsigned n0 = __byte_perm(pw, w0, 0x5432), n1 = __byte_perm(w0, w1, 0x5432);
+            *reinterpret_cast<unsigned *>(drow + 2) = n1;
+            if (lane != 0) *reinterpret_cast<unsigned *>(drow) = n0;
+            else h[1] = (unsigned short)(w0 & 0xffffu);
+            if (lane == 31) h[4] = (unsigned short)(w1 >> 16);
+        } else if (LBGPU_AA4_ODD_SPLIT) {
+            const unsigned nw = __shfl_down_sync(0xffffffffu, w0, 1);
+            const unsigned n0 = __byte_perm(w0, w1, 0x5432), n1 = __byte_perm(w1, nw, 0x5432);
+            *reinterpret_cast<unsigned *>(drow) = n0;
+            if (lane != 31) *reinterpret_cast<unsigned *>(drow + 2) = n1;
+            else h[2] = (unsigned short)(w1 >> 16);
+            if (lane == 0) h[-1] = (unsigned short)(w0 & 0xffffu);
         } else if (cx(i) == 1) {     // positions x0..x0+3 take nodes x0-1 (previous lane), x0, x0+1, x0+2
             const unsigned pw = __shfl_up_sync(0xffffffffu, w1, 1);
             const unsigned n0 = __byte_perm(pw, w0, 0x5432), n1 = __byte_perm(w0, w1, 0x5432);
