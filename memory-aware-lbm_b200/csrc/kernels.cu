@@ -847,6 +847,10 @@ __device__ __forceinline__ void walk_hold(typename Work<S>::W up_next[3], typena
 
 // Rows ahead of the walk prefetched into L2 (0: none), measured on the 16384 x 4096 channel
 // (GLUPS of two steps per sweep at 0 / 4 / 8 rows): FP64 29.7 / 38.8 / 33.3, FP32 77.3 / 62.1 / 62.0.
+#ifndef LBGPU_SWEEP2W_UNROLL
+#define LBGPU_SWEEP2W_UNROLL 1     // rows of the walk a loop iteration holds
+#endif
+constexpr int kSweep2wUnroll = LBGPU_SWEEP2W_UNROLL;
 #ifndef LBGPU_SWEEP2W_PF64
 #define LBGPU_SWEEP2W_PF64 4
 #endif
@@ -902,6 +906,7 @@ __global__ void __launch_bounds__(128, sweep2w_min_blocks<S>()) k_sweep2w(Geo g,
         }
     };
     fetch(y0 - 2);
+#pragma unroll kSweep2wUnroll
     for (int R = y0 - 2; R <= yend + 1; ++R) {
         // C_n row R, lane-shifted
         W cur[9];
