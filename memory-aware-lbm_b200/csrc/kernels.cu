@@ -156,23 +156,24 @@ __device__ __forceinline__ void bgk_offsets(float D[9], float omega, float sc, f
     const float ux = SHIFT ? fmaf(Jx, q, __fmul_rn(us, ir)) : Jx * q, uy = Jy * q;
     float A = fmaf(-1.5f * inv, fmaf(Jx, ux, Jy * uy), d);
     // shifted terms: t = ux - us; 4.5 (c.us)(c.u - c.us) is e1 = 4.5 us t for (1, 3) and
-    // e1 +- 4.5 us uy for (5, 7) and (6, 8)
+    // e1 +- 4.5 us uy for (5, 7) and (6, 8), folded into the pair's constant term: A1 = A + e1,
+    // A1 +- 4.5 us uy
     const float t = SHIFT ? __fsub_rn(ux, us) : 0.0f;
     if (SHIFT) A = fmaf(-1.5f * us, t, A);
     const float ux45 = (4.5f * inv) * ux, uy45 = (4.5f * inv) * uy;
     const float hs = 4.5f * us;
-    const float e1 = SHIFT ? __fmul_rn(hs, t) : 0.0f, ev = SHIFT ? __fmul_rn(hs, uy) : 0.0f;
+    const float A1 = SHIFT ? fmaf(hs, t, A) : A, ev = SHIFT ? __fmul_rn(hs, uy) : 0.0f;
+    const float A5 = SHIFT ? __fadd_rn(A1, ev) : A, A6 = SHIFT ? __fsub_rn(A1, ev) : A;
     const float om1 = 1.0f - omega;
     const float k0 = omega * sc * (4.f / 9.f), k1 = omega * sc * (1.f / 9.f), k2 = omega * sc * (1.f / 36.f);
     D[0] = fmaf(om1, D[0], k0 * A);
     // The shifted terms use explicitly rounded operations: no multiply-add contraction may
     // differ between the kernels that inline this, so every scheme stays bit-identical.
-#define LBGPU_PAIR(I, J, K, CU45, CJ, EXTRA, HAS_EXTRA)                \
+#define LBGPU_PAIR(I, J, K, CU45, CJ, AP)                              \
     {                                                                  \
         const float cj = (CJ);                                         \
         if (SHIFT) {                                                   \
-            const float a0 = fmaf(CU45, cj, A);                        \
-            const float a = __fmul_rn(K, HAS_EXTRA ? __fadd_rn(a0, (EXTRA)) : a0); \
+            const float a = __fmul_rn(K, fmaf(CU45, cj, (AP)));        \
             const float b = __fmul_rn((3.0f * inv) * K, cj);          \
             D[I] = fmaf(om1, D[I], __fadd_rn(a, b));                   \
             D[J] = fmaf(om1, D[J], __fsub_rn(a, b));                   \
@@ -183,10 +184,10 @@ __device__ __forceinline__ void bgk_offsets(float D[9], float omega, float sc, f
             D[J] = fmaf(om1, D[J], a - b);                             \
         }                                                              \
     }
-    LBGPU_PAIR(1, 3, k1, ux45, Jx, e1, true)
-    LBGPU_PAIR(2, 4, k1, uy45, Jy, 0.0f, false)
-    LBGPU_PAIR(5, 7, k2, __fadd_rn(ux45, uy45), __fadd_rn(Jx, Jy), __fadd_rn(e1, ev), true)
-    LBGPU_PAIR(6, 8, k2, __fsub_rn(uy45, ux45), __fsub_rn(Jy, Jx), __fsub_rn(e1, ev), true)
+    LBGPU_PAIR(1, 3, k1, ux45, Jx, A1)
+    LBGPU_PAIR(2, 4, k1, uy45, Jy, A)
+    LBGPU_PAIR(5, 7, k2, __fadd_rn(ux45, uy45), __fadd_rn(Jx, Jy), A5)
+    LBGPU_PAIR(6, 8, k2, __fsub_rn(uy45, ux45), __fsub_rn(Jy, Jx), A6)
 #undef LBGPU_PAIR
 }
 
