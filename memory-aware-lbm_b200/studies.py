@@ -199,6 +199,13 @@ def _serve(prec, reqs, batched, budget, schemes=None, shapes=None, sample=(), sh
             "diverged": sum(1 for r in res if r["converged"] == -1)}, res
 
 
+def _progress(tag, obj):
+    """One JSON line per finished part on stderr, so a long study's parts survive its end."""
+    import json
+    import sys
+    print(json.dumps({"part": tag, **obj}), file=sys.stderr, flush=True)
+
+
 def serving_study(precisions=("f32", "f16"), n=5000, seed=20260102, budget_gb=150.0,
                   load=0.95, sample_every=50, shift=0, rs=0, calib=400, plain_every=10,
                   solo_nodes=-1):
@@ -207,7 +214,8 @@ def serving_study(precisions=("f32", "f16"), n=5000, seed=20260102, budget_gb=15
     times that rate are then served batched and sequentially (plain solves one at a time, the
     same storage), the same stream for both.  A 2 % sample (every `sample_every`-th request) is
     re-run alone in FP64 for the velocity error; sequential FP64 plain solves of every
-    `plain_every`-th request give the FP64 plain rate.  shift=1: 16-bit requests store offsets
+    `plain_every`-th request give the FP64 plain rate (plain_every=0 skips them; precisions=none
+    runs them alone, so the parts fit separate runs).  shift=1: 16-bit requests store offsets
     from their inflow profile; rs=1: they round stochastically.  solo_nodes >= 0 overrides the
     server's size above which a request steps on its own (0: every request in the batch)."""
     reqs = serving_requests(n, seed)
@@ -224,17 +232,21 @@ def serving_study(precisions=("f32", "f16"), n=5000, seed=20260102, budget_gb=15
            "fp64_sample": len(sample), "precisions": {}}
     rng = np.random.default_rng(seed + 1)
     mean_work = float(np.mean(work))
+    precisions = tuple(p for p in precisions if p != "none")
     for prec in precisions:
         schemes = {c: v["scheme"] for c, v in
                    tune_schemes(prec, [(q["lx"], q["ly"]) for q in reqs]).items()}
         head = reqs[:calib]
         closed, _ = _serve(prec, head, True, budget, schemes, shift=shift, rs=rs, solo_nodes=solo)
+        _progress(f"{prec} calibration", closed)
         rate = load * closed["mlups"] * 1e6 / mean_work            # requests per second
         t = np.cumsum(rng.exponential(1.0 / rate, n))
         stream = [dict(q, arrival=float(t[k] - t[0])) for k, q in enumerate(reqs)]
         served, res = _serve(prec, stream, True, budget, schemes, sample=sample, shift=shift, rs=rs,
                              solo_nodes=solo)
+        _progress(f"{prec} stream batched", served)
         seq, _ = _serve(prec, stream, False, budget, shift=shift, rs=rs)
+        _progress(f"{prec} stream sequential", seq)
         errs, detail = [], []
         for k in sorted(sample):
             q = reqs[k]
@@ -267,14 +279,17 @@ def serving_study(precisions=("f32", "f16"), n=5000, seed=20260102, budget_gb=15
                                         "at_umax_cap": {"n": len(capped), "median": _pct(capped, 50),
                                                         "max": max(capped) if capped else None},
                                         "requests": detail}}
+        _progress(f"{prec} result", out["precisions"][prec])
     # sequential plain FP64 solves of every plain_every-th request, all present at t = 0
-    sub = reqs[::plain_every]
-    plain, _ = _serve("f64", sub, False, budget)
-    out["sequential_f64_plain"] = dict(plain, requests=len(sub))
-    for prec in precisions:
-        p = out["precisions"][prec]
-        p["throughput_ratio_vs_f64_plain"] = round(p["stream_batched"]["mlups_not_diverged"] /
-                                                   max(plain["mlups_not_diverged"], 1e-9), 2)
+    if plain_every:
+        sub = reqs[::plain_every]
+        plain, _ = _serve("f64", sub, False, budget)
+        _progress("f64 plain", plain)
+        out["sequential_f64_plain"] = dict(plain, requests=len(sub))
+        for prec in precisions:
+            p = out["precisions"][prec]
+            p["throughput_ratio_vs_f64_plain"] = round(p["stream_batched"]["mlups_not_diverged"] /
+                                                       max(plain["mlups_not_diverged"], 1e-9), 2)
     return out
 
 
