@@ -173,3 +173,59 @@ def test_batch_rejects_mismatched_members():
 def test_scheme_tuner_reports_both_timings():
     scheme, t_pull, t_aa = lbgpu.tune_scheme("f32", 512, 128, 6)
     assert scheme in ("pull", "aa") and t_pull > 0 and t_aa > 0
+
+
+@pytest.mark.parametrize("precision,passes", [("f32", 1), ("f32", 3), ("f16", 64), ("bf16", 3)])
+def test_strip_lengths_are_exact(precision, passes):
+    """A block stepping `passes` tiles down a member gives the same result for every strip
+    length, ragged member heights included (the last strip of a member stops at its last row)."""
+    schemes = ["pull", "aa", "pull", "pull", "aa", "pull"]
+    steps = 57
+    lats = [channel(lx, ly, precision, s, k) for k, ((lx, ly), s) in enumerate(zip(SIZES, schemes))]
+    with lbgpu.Batch(precision) as b:
+        for c in range(6):
+            b.set_passes(c, passes)
+            assert b.passes(c) == passes
+            if precision != "f32":
+                b.set_shape(c, 128, 4)
+        for l in lats:
+            b.add(l)
+        b.step(steps)
+        b.synchronize()
+        got = [l.populations() for l in lats]
+    for k, ((lx, ly), s) in enumerate(zip(SIZES, schemes)):
+        assert same(got[k], alone(lx, ly, precision, s, k, steps)), (precision, passes, k, s)
+    for l in lats:
+        l.close()
+
+
+def test_row_shifted_member_in_a_quad_batch_is_exact():
+    """A 16-bit member with offsets from a banded inflow profile (the batch then runs the quad
+    kernel with the shifted path) next to unshifted members: each as stepped alone."""
+    steps = 53
+
+    def make(k, lx, ly, shifted):
+        lat = channel(lx, ly, "f16", "pull", k) if not shifted else None
+        if shifted:
+            lat = lbgpu.Lattice(lx, ly, "f16", "pull")
+            lbgpu.configure_storage(lat, "f16br", 0.03, seed=7)
+            lat.setup_cylinder(lx // 5 + 1, ly // 2 + 1, ly // 10 + 1, 0.03, 120.0,
+                               lbgpu.WALL_BOUNCEBACK, lbgpu.OUTLET_CONST)
+        return lat
+
+    spec = [(0, 200, 64, True), (1, 257, 135, False), (2, 130, 70, True)]
+    lats = [make(*q) for q in spec]
+    with lbgpu.Batch("f16") as b:
+        for c in range(6):
+            b.set_shape(c, 128, 4)
+        for l in lats:
+            b.add(l)
+        b.step(steps)
+        b.synchronize()
+        got = [l.populations() for l in lats]
+    for (k, lx, ly, shifted), g in zip(spec, got):
+        with make(k, lx, ly, shifted) as lat:
+            lat.step(steps)
+            assert same(g, lat.populations()), (k, shifted)
+    for l in lats:
+        l.close()
