@@ -848,10 +848,6 @@ __device__ __forceinline__ void walk_hold(typename Work<S>::W up_next[3], typena
 
 // Rows ahead of the walk prefetched into L2 (0: none), measured on the 16384 x 4096 channel
 // (GLUPS of two steps per sweep at 0 / 4 / 8 rows): FP64 29.7 / 38.8 / 33.3, FP32 77.3 / 62.1 / 62.0.
-#ifndef LBGPU_SWEEP2W_UNROLL
-#define LBGPU_SWEEP2W_UNROLL 1     // rows of the walk a loop iteration holds
-#endif
-constexpr int kSweep2wUnroll = LBGPU_SWEEP2W_UNROLL;
 #ifndef LBGPU_SWEEP2W_PF64
 #define LBGPU_SWEEP2W_PF64 4
 #endif
@@ -907,7 +903,6 @@ __global__ void __launch_bounds__(128, sweep2w_min_blocks<S>()) k_sweep2w(Geo g,
         }
     };
     fetch(y0 - 2);
-#pragma unroll kSweep2wUnroll
     for (int R = y0 - 2; R <= yend + 1; ++R) {
         // C_n row R, lane-shifted
         W cur[9];
@@ -1173,9 +1168,6 @@ __global__ void __launch_bounds__(BX, SHIFT ? 7 : 8) k_aa4_even(Geo g, S *__rest
     for (int i = 0; i < 9; ++i) *reinterpret_cast<uint2 *>(plane(a, g, opp(i)) + o) = pack_quad<S, RS>(D, i, hq);
 }
 
-#ifndef LBGPU_AA4_ODD_SPLIT
-#define LBGPU_AA4_ODD_SPLIT 0       // 1: shifted word pairs stored as two 4-byte halves
-#endif
 #ifndef LBGPU_AA4_ODD_MINB
 #define LBGPU_AA4_ODD_MINB 7        // resident blocks of the odd AA step (72 registers)
 #endif
@@ -1224,20 +1216,6 @@ __global__ void __launch_bounds__(BX, SHIFT ? LBGPU_AA4_ODD_MINB - 1 : LBGPU_AA4
         unsigned short *h = reinterpret_cast<unsigned short *>(drow);
         if (cx(i) == 0) {
             *reinterpret_cast<uint2 *>(drow) = make_uint2(w0, w1);
-        } else if (LBGPU_AA4_ODD_SPLIT && cx(i) == 1) {   // as below, every branch a single store
-            const unsigned pw = __shfl_up_sync(0xffffffffu, w1, 1);
-            const unsigned n0 = __byte_perm(pw, w0, 0x5432), n1 = __byte_perm(w0, w1, 0x5432);
-            *reinterpret_cast<unsigned *>(drow + 2) = n1;
-            if (lane != 0) *reinterpret_cast<unsigned *>(drow) = n0;
-            else h[1] = (unsigned short)(w0 & 0xffffu);
-            if (lane == 31) h[4] = (unsigned short)(w1 >> 16);
-        } else if (LBGPU_AA4_ODD_SPLIT) {
-            const unsigned nw = __shfl_down_sync(0xffffffffu, w0, 1);
-            const unsigned n0 = __byte_perm(w0, w1, 0x5432), n1 = __byte_perm(w1, nw, 0x5432);
-            *reinterpret_cast<unsigned *>(drow) = n0;
-            if (lane != 31) *reinterpret_cast<unsigned *>(drow + 2) = n1;
-            else h[2] = (unsigned short)(w1 >> 16);
-            if (lane == 0) h[-1] = (unsigned short)(w0 & 0xffffu);
         } else if (cx(i) == 1) {     // positions x0..x0+3 take nodes x0-1 (previous lane), x0, x0+1, x0+2
             const unsigned pw = __shfl_up_sync(0xffffffffu, w1, 1);
             const unsigned n0 = __byte_perm(pw, w0, 0x5432), n1 = __byte_perm(w0, w1, 0x5432);
@@ -1299,13 +1277,13 @@ constexpr int batch_min_blocks()
     return b128 * 128 / BT > 0 ? b128 * 128 / BT : 1;
 }
 
-// RS: the kernel also serves stochastically rounded members (16-bit only); batches without
-// any keep kernels without that code, whose registers it would otherwise raise.
 // One strip of tiles (BatchWork): the member's descriptor is read once, then the block walks its
 // passes down the lattice; every node runs the single-lattice node function.  With
 // LBGPU_BATCH_PF > 0 the rows of the tile that many passes ahead are prefetched into L2 at the
 // start of each pass (lane 0 of each warp for the warp's row segment, with prefetch_rows_l2's
-// alignment and bounds rules: tile widths and x0 - 1 are multiples of 32 nodes).
+// alignment and bounds rules: tile widths and x0 - 1 are multiples of 32 nodes).  Off by
+// default: one and two passes ahead measured slower on the 512-channel mix (FP32 60-66 against
+// 66-75 GLUPS, FP16 80-100 against 85-97).
 #ifndef LBGPU_BATCH_PF
 #define LBGPU_BATCH_PF 0
 #endif
