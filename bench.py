@@ -357,7 +357,7 @@ def run_ours(args, dist):
     if args.variants == "auto":
         vlist = [("f64", "aa"), ("f64", "pull2"), ("f32", "pull"), ("f32", "aa"), ("f32", "pull2"),
                  ("f16", "pull"), ("bf16", "pull"), ("f16", "aa"), ("f16", "pull2"),
-                 ("f16r", "pull"), ("f16sr", "pull"), ("f16r", "aa")]
+                 ("f16r", "pull"), ("f16sr", "pull"), ("f16br", "pull"), ("f16r", "aa")]
     elif args.variants != "none":
         vlist = [tuple(v.split(":")) for v in args.variants.split(",") if v]
     for prec, sch in vlist:
