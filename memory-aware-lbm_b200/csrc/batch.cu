@@ -30,7 +30,8 @@ namespace {
 
 constexpr int kClasses = 6;     // node-count classes: < 16K, 64K, 256K, 1M, 4M, above
 constexpr int kChunk = 50;      // steps per captured graph (even: buffer parities repeat)
-constexpr int kLists = 4;       // pull, pull four nodes a thread; AA of phase parity 0, 1 at rebuild
+constexpr int kLists = 5;       // pull, pull four nodes a thread; AA of phase parity 0, 1 at rebuild;
+                                // the perimeters of the four-nodes-a-thread members
 constexpr int kQuad = 3;        // shape of the four-nodes-a-thread pull tiles (16-bit storage)
 constexpr int kMaxPasses = 64;  // tiles a block may step down one member
 
@@ -58,10 +59,10 @@ struct lbgpu_batch {
     bool persistent = false;
     BatchInst *d_inst = nullptr;
     int cap_inst = 0;
-    BatchWork *d_work[kLists] = {nullptr, nullptr, nullptr, nullptr};
-    int cap_work[kLists] = {0, 0, 0, 0};
-    int nwork[kLists] = {0, 0, 0, 0};
-    int per_sm[4][3] = {};                   // resident blocks per SM, [kind][threads 128/256/512]
+    BatchWork *d_work[kLists] = {};
+    int cap_work[kLists] = {};
+    int nwork[kLists] = {};
+    int per_sm[lbgpu::BATCH_KINDS][3] = {};  // resident blocks per SM, [kind][threads 128/256/512]
     int sms = 0;
     int aa_phase = 0;                        // phase parity of list 2 now (list 3: the other)
     std::vector<BatchInst> h_inst;
@@ -186,6 +187,7 @@ int rebuild(lbgpu_batch *b)
         for (int y0 = 1; y0 <= L.ly; y0 += th)
             for (int x0 = 1; x0 <= L.lx; x0 += tw)
                 work[s].push_back(BatchWork{(int)i, x0, y0, lbgpu::batch_sp(sh, np)});
+        if (s == 1) work[4].push_back(BatchWork{(int)i, 1, 1, lbgpu::batch_sp(sh, 1)});   // its perimeter
     }
     b->aa_phase = 0;
     b->rs = false;
@@ -214,7 +216,7 @@ int rebuild(lbgpu_batch *b)
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
-        for (int kind = 0; kind < 4; ++kind)
+        for (int kind = 0; kind < lbgpu::BATCH_KINDS; ++kind)
             for (int t = 0; t < 3; ++t)
                 b->per_sm[kind][t] = std::max(1, lbgpu::batch_blocks_per_sm(b->precision, kind, 128 << t));
     }
@@ -228,8 +230,8 @@ void launch_step(lbgpu_batch *b, int k)
 {
     for (int s = 0; s < kLists; ++s) {
         if (!b->nwork[s]) continue;
-        int kind = s == 0 ? lbgpu::BATCH_PULL : lbgpu::BATCH_PULL4;
-        if (s >= 2) {
+        int kind = s == 0 ? lbgpu::BATCH_PULL : (s == 1 ? lbgpu::BATCH_PULL4 : lbgpu::BATCH_PERIM);
+        if (s == 2 || s == 3) {
             const int phase = (s == 2) ? b->aa_phase : 1 - b->aa_phase;
             kind = ((phase + k) & 1) ? lbgpu::BATCH_AA_ODD : lbgpu::BATCH_AA_EVEN;
         }

@@ -513,6 +513,31 @@ __device__ __forceinline__ void pull_node(const Geo &g, const S *__restrict__ sr
     }
 }
 
+// Perimeter node number p (Geo::pidx numbering: row 1, row ly, then columns 1 and lx without
+// their corners) -> its coordinates; false for numbers that name no node, or a node a second
+// time where the lattice is one row or one column wide.
+__device__ __forceinline__ bool perim_node(const Geo &g, int p, int &X, int &Y)
+{
+    if (p < g.lx) { X = p + 1; Y = 1; return true; }
+    if (p < 2 * g.lx) { X = p - g.lx + 1; Y = g.ly; return g.ly > 1; }
+    const int q = p - 2 * g.lx;
+    if (q < g.ly - 2) { X = 1; Y = q + 2; return true; }
+    if (q >= g.ly && q < 2 * g.ly - 2) { X = g.lx; Y = q - g.ly + 2; return g.lx > 1; }
+    return false;
+}
+
+// The pull step of every perimeter node, one a thread (the 16-bit quad kernels leave them out,
+// see pull_quad's PERIM_APART).
+template <class S, int SH, bool RS>
+__global__ void __launch_bounds__(256) k_perim_pull(Geo g, const S *__restrict__ src, S *__restrict__ dst,
+                                                    const uint8_t *__restrict__ tag, const double *__restrict__ bc,
+                                                    double omega, S *__restrict__ side, float sc, float inv)
+{
+    int X, Y;
+    if (perim_node(g, (int)(blockIdx.x * 256 + threadIdx.x), X, Y))
+        pull_node<S, SH, RS>(g, src, dst, tag, bc, omega, side, sc, inv, X, Y, g.rs_key);
+}
+
 // The hash of the quad x0..x0+3 (RS only).
 template <class S, bool RS>
 __device__ __forceinline__ unsigned quad_hash(const Geo &g, unsigned key, int x0, int Y)
@@ -551,7 +576,10 @@ __device__ __forceinline__ uint2 pack_quad(const float D[4][9], int i, unsigned 
 // vector loads of an edge quad stay inside the allocation: left of column 1 they reach the row
 // padding and ghost column (x0 - 2 >= -1), past lx they reach at most five elements into the
 // row padding or the next row, which exists because Y <= ly - 1.
-template <class S, bool SHIFT, bool RS = false>
+// PERIM_APART: the perimeter nodes are stepped by another kernel (the batch's BATCH_PERIM
+// list): rows 1 and ly are skipped, and an edge quad stores its inner nodes only, so no lane of
+// a quad warp runs the per-node path while the others wait.
+template <class S, bool SHIFT, bool RS = false, bool PERIM_APART = false>
 __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ src, S *__restrict__ dst,
                                           const uint8_t *__restrict__ tag, const double *__restrict__ bc,
                                           double omega, S *__restrict__ side, float sc, float inv, int x0,
@@ -560,8 +588,10 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
     using H = Half2Ops<S>;
     (void)lane;
     if (Y < 2 || Y > g.ly - 1) {
-        for (int k = 0; k < 4; ++k)
-            if (x0 + k <= g.lx) pull_node<S, SHIFT ? 1 : 0, RS>(g, src, dst, tag, bc, omega, side, sc, inv, x0 + k, Y, key);
+        if constexpr (!PERIM_APART) {
+            for (int k = 0; k < 4; ++k)
+                if (x0 + k <= g.lx) pull_node<S, SHIFT ? 1 : 0, RS>(g, src, dst, tag, bc, omega, side, sc, inv, x0 + k, Y, key);
+        }
         return;
     }
     if (x0 > g.lx) return;
@@ -620,12 +650,16 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
 #pragma unroll
             for (int i = 0; i < 9; ++i) plane(dst, g, i)[o + k] = put<S, RS>(D[k][i], i, sc, RsNode{hq, k});
         }
+        if constexpr (PERIM_APART) return;
         if (x0 == 1) pull_node<S, SHIFT ? 1 : 0, RS>(g, src, dst, tag, bc, omega, side, sc, inv, 1, Y, key);
         if (g.lx >= x0 && g.lx <= x0 + 3 && g.lx >= 2)
             pull_node<S, SHIFT ? 1 : 0, RS>(g, src, dst, tag, bc, omega, side, sc, inv, g.lx, Y, key);
     }
 }
 
+#ifndef LBGPU_PULL4H_PERIM_APART
+#define LBGPU_PULL4H_PERIM_APART 1  // perimeter nodes stepped by k_perim_pull after k_pull4h
+#endif
 #ifndef LBGPU_PULL4H_SHIFT_MINB
 #define LBGPU_PULL4H_SHIFT_MINB 7   // resident blocks of the row-shifted form (72 registers)
 #endif
@@ -639,8 +673,8 @@ __global__ void __launch_bounds__(BX, SHIFT ? LBGPU_PULL4H_SHIFT_MINB : 8) k_pul
         prefetch_rows_l2<S, 4 * BX>(g, src, 1 + 4 * BX * (int)blockIdx.x, (int)blockIdx.y + 1 + LBGPU_PF_ROWS,
                                     LBGPU_PF_TAGS ? tag : nullptr);
     const int t = blockIdx.x * BX + threadIdx.x;
-    pull_quad<S, SHIFT, RS>(g, src, dst, tag, bc, omega, side, sc, inv, 1 + 4 * t, blockIdx.y + 1, threadIdx.x & 31,
-                            g.rs_key);
+    pull_quad<S, SHIFT, RS, LBGPU_PULL4H_PERIM_APART != 0>(g, src, dst, tag, bc, omega, side, sc, inv, 1 + 4 * t,
+                                                          blockIdx.y + 1, threadIdx.x & 31, g.rs_key);
 }
 
 // Propagation of C_n in `src` into `dst` (form C -> form L), ghost ring included; stale
@@ -1273,6 +1307,7 @@ constexpr int batch_min_blocks()
     else if (KIND == BATCH_PULL) b128 = PERSIST ? 8 : 16;
     else if (KIND == BATCH_AA_EVEN) b128 = PERSIST ? 8 : 10;
     else if (KIND == BATCH_PULL4) b128 = LBGPU_PULL4_MINB;
+    else if (KIND == BATCH_PERIM) b128 = 8;
     else b128 = (sizeof(S) == 4 && !PERSIST) ? 6 : 8;
     return b128 * 128 / BT > 0 ? b128 * 128 / BT : 1;
 }
@@ -1321,12 +1356,35 @@ __device__ __forceinline__ void batch_strip(const BatchInst *__restrict__ insts,
                 if (LBGPU_BATCH_PF > 0 && lane == 0 && p + LBGPU_BATCH_PF < passes)
                     batch_prefetch<S, 128, 0>(g, sb, it.x0, Y + LBGPU_BATCH_PF * (BT / 32), d.tag);
                 if (RS && rs) {
-                    if (SHQ && g.shift_u) pull_quad<S, true, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane, key);
-                    else pull_quad<S, false, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane, key);
+                    if (SHQ && g.shift_u) pull_quad<S, true, true, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane, key);
+                    else pull_quad<S, false, true, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane, key);
                 } else if (SHQ && g.shift_u) {
-                    pull_quad<S, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane);
+                    pull_quad<S, true, false, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane);
                 } else {
-                    pull_quad<S, false>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane);
+                    pull_quad<S, false, false, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, x0, Y, lane);
+                }
+            }
+        }
+        return;
+    }
+    if constexpr (KIND == BATCH_PERIM) {
+        if constexpr (sizeof(S) == 2) {
+            // the member's perimeter (perim_node numbering)
+            const int src = d.cur0 ^ (k & 1);
+            const S *sb = static_cast<const S *>(d.buf[src]);
+            S *db = static_cast<S *>(d.buf[src ^ 1]);
+            const bool rs = RS && d.rs;
+            const unsigned key = rs ? rs_key(d.rs_seed, (unsigned long long)(d.tau0 + k)) : 0u;
+            for (int p = threadIdx.x; p < 2 * g.lx + 2 * g.ly; p += BT) {
+                int X, Y;
+                if (!perim_node(g, p, X, Y)) continue;
+                if (RS && rs) {
+                    if (SHQ && g.shift_u) pull_node<S, 1, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, X, Y, key);
+                    else pull_node<S, 0, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, X, Y, key);
+                } else if (SHQ && g.shift_u) {
+                    pull_node<S, 1>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, X, Y);
+                } else {
+                    pull_node<S, 0>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, X, Y);
                 }
             }
         }
@@ -1778,6 +1836,9 @@ static void launch_pull4h_t(const DevLattice &d, dim3 grid, int src, int side_pa
 {
     k_pull4h<S, SHIFT, RS><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
                                                SIDE<S>(d, side_par), d.scale, d.inv_scale);
+    if (LBGPU_PULL4H_PERIM_APART)
+        k_perim_pull<S, SHIFT ? 1 : 0, RS><<<cdiv(2 * d.g.lx + 2 * d.g.ly, 256), 256, 0, s>>>(
+            d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega, SIDE<S>(d, side_par), d.scale, d.inv_scale);
 }
 
 template <class S>
@@ -1790,6 +1851,12 @@ static void launch_pull4h(const DevLattice &d, dim3 grid, int src, int side_par,
         if (d.g.rs_key) launch_pull4h_t<S, false, true>(d, grid, src, side_par, s);
         else launch_pull4h_t<S, false, false>(d, grid, src, side_par, s);
     }
+}
+
+int pull_launches(const DevLattice &d, bool ghosts)
+{
+    const bool half = d.precision == LBGPU_F16 || d.precision == LBGPU_BF16;
+    return (!ghosts && half && LBGPU_PULL4H_PERIM_APART) ? 2 : 1;
 }
 
 void launch_pull(const DevLattice &d, int src, int side_par, bool ghosts, cudaStream_t s)
@@ -1943,9 +2010,9 @@ static void launch_batch_b(bool persistent, int flags, const BatchInst *insts, c
                            int grid, int k, cudaStream_t s)
 {
     if constexpr (sizeof(S) == 2) {
-        const int f = KIND == BATCH_PULL4 ? (flags & 3) : (flags & 1);
+        const int f = (KIND == BATCH_PULL4 || KIND == BATCH_PERIM) ? (flags & 3) : (flags & 1);
         if (f == 1) return launch_batch_r<S, KIND, BT, 1>(persistent, insts, work, nwork, grid, k, s);
-        if constexpr (KIND == BATCH_PULL4) {
+        if constexpr (KIND == BATCH_PULL4 || KIND == BATCH_PERIM) {
             if (f == 2) return launch_batch_r<S, KIND, BT, 2>(persistent, insts, work, nwork, grid, k, s);
             if (f == 3) return launch_batch_r<S, KIND, BT, 3>(persistent, insts, work, nwork, grid, k, s);
         }
@@ -1971,8 +2038,10 @@ static void launch_batch_t(int kind, int bt, bool persistent, int rs, const Batc
         launch_batch_k<S, BATCH_AA_EVEN>(bt, persistent, rs, insts, work, nwork, grid, k, s);
     else if (kind == BATCH_AA_ODD)
         launch_batch_k<S, BATCH_AA_ODD>(bt, persistent, rs, insts, work, nwork, grid, k, s);
-    else if constexpr (sizeof(S) == 2)
-        launch_batch_k<S, BATCH_PULL4>(bt, persistent, rs, insts, work, nwork, grid, k, s);
+    else if constexpr (sizeof(S) == 2) {
+        if (kind == BATCH_PULL4) launch_batch_k<S, BATCH_PULL4>(bt, persistent, rs, insts, work, nwork, grid, k, s);
+        else launch_batch_k<S, BATCH_PERIM>(bt, persistent, rs, insts, work, nwork, grid, k, s);
+    }
 }
 
 void launch_batch(int precision, int kind, int threads, bool persistent, int rs, const BatchInst *insts,
@@ -2002,7 +2071,10 @@ static int blocks_t(int kind, int bt)
     if (kind == BATCH_PULL) return blocks_k<S, BATCH_PULL>(bt);
     if (kind == BATCH_AA_EVEN) return blocks_k<S, BATCH_AA_EVEN>(bt);
     if (kind == BATCH_AA_ODD) return blocks_k<S, BATCH_AA_ODD>(bt);
-    if constexpr (sizeof(S) == 2) return blocks_k<S, BATCH_PULL4>(bt);
+    if constexpr (sizeof(S) == 2) {
+        if (kind == BATCH_PULL4) return blocks_k<S, BATCH_PULL4>(bt);
+        return blocks_k<S, BATCH_PERIM>(bt);
+    }
     return 0;
 }
 

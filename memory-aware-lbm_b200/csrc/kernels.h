@@ -30,6 +30,9 @@ enum { VIEW_DIRECT = 0, VIEW_PULL_PENDING = 1, VIEW_AA_NATURAL = 2, VIEW_AA_SWAP
 
 void launch_collide_inplace(const DevLattice &d, int cur, int side_par, cudaStream_t s);
 void launch_pull(const DevLattice &d, int src, int side_par, bool ghosts, cudaStream_t s);
+// Kernels launch_pull launches (16-bit storage without the ghost ring: the quad kernel and the
+// perimeter kernel).
+int pull_launches(const DevLattice &d, bool ghosts);
 void launch_stream(const DevLattice &d, int src, int side_par, cudaStream_t s);
 // Two pull steps in one sweep (temporal blocking): C_n in buffer src (n_par = n & 1) ->
 // C_{n+2} in buffer 1 - src, then the stale-slot scratch into parity n+1 and the two buffers'
@@ -68,9 +71,12 @@ void launch_velocity_change(const DevLattice &d, int view, int cur, int side_par
                             unsigned *out, cudaStream_t s);
 // ---- batches: many lattices per launch ------------------------------------------------
 // threads per block = nodes per tile: 128, 256 or 512
-// Kinds of batch step: pull (one node per thread), AA even and odd, and the 16-bit pull with four
-// nodes per thread (each warp one row of 128 nodes, see pull_quad).
-enum { BATCH_PULL = 0, BATCH_AA_EVEN = 1, BATCH_AA_ODD = 2, BATCH_PULL4 = 3 };
+// Kinds of batch step: pull (one node per thread), AA even and odd, the 16-bit pull with four
+// nodes per thread (each warp one row of 128 nodes, see pull_quad), which leaves each member's
+// perimeter nodes to BATCH_PERIM: the pull step of those nodes, one per thread, one block a
+// member (work item: the member; its block loops over the perimeter).
+enum { BATCH_PULL = 0, BATCH_AA_EVEN = 1, BATCH_AA_ODD = 2, BATCH_PULL4 = 3, BATCH_PERIM = 4 };
+constexpr int BATCH_KINDS = 5;
 
 // One lattice of a batch, with its state at the start of the current chunk of steps:
 // pull scheme: the buffer holding C_n is buf[cur0]; AA: phase0 0 = natural form, 1 = swapped;

@@ -172,6 +172,7 @@ int Lattice::op_collide()
     if (form == FORM_C && pending) {
         set_rs_keys(n + 1);
         launch_pull(d, cur, (int)((n + 1) & 1), ghosts, stream);
+        launches += pull_launches(d, ghosts) - 1;
         cur = 1 - cur;
         ++n;
     } else {
