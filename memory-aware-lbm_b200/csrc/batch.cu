@@ -187,7 +187,9 @@ int rebuild(lbgpu_batch *b)
         for (int y0 = 1; y0 <= L.ly; y0 += th)
             for (int x0 = 1; x0 <= L.lx; x0 += tw)
                 work[s].push_back(BatchWork{(int)i, x0, y0, lbgpu::batch_sp(sh, np)});
-        if (s == 1) work[4].push_back(BatchWork{(int)i, 1, 1, lbgpu::batch_sp(sh, 1)});   // its perimeter
+        if (s == 1)   // its perimeter, one block a run of `threads` perimeter nodes
+            for (int p0 = 0; p0 < 2 * L.lx + 2 * L.ly; p0 += b->threads)
+                work[4].push_back(BatchWork{(int)i, p0, 1, lbgpu::batch_sp(sh, 1)});
     }
     b->aa_phase = 0;
     b->rs = false;

@@ -658,12 +658,15 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
 }
 
 #ifndef LBGPU_PULL4H_PERIM_APART
-#define LBGPU_PULL4H_PERIM_APART 1  // perimeter nodes stepped by k_perim_pull after k_pull4h
+#define LBGPU_PULL4H_PERIM_APART 1  // perimeter nodes stepped apart from the quads (see k_pull4h)
 #endif
 #ifndef LBGPU_PULL4H_SHIFT_MINB
 #define LBGPU_PULL4H_SHIFT_MINB 7   // resident blocks of the row-shifted form (72 registers)
 #endif
-template <class S, bool SHIFT, bool RS>
+// PERIM_APART: the quads leave the perimeter to another pass (see pull_quad); PERIM_ROWS: that pass
+// is the grid rows past the lattice's ly rows, one perimeter node a thread, so it runs inside the
+// same launch (in its tail) instead of as a launch of its own.
+template <class S, bool SHIFT, bool RS, bool PERIM_APART = false, bool PERIM_ROWS = false>
 __global__ void __launch_bounds__(BX, SHIFT ? LBGPU_PULL4H_SHIFT_MINB : 8) k_pull4h(Geo g, const S *__restrict__ src, S *__restrict__ dst,
                                                const uint8_t *__restrict__ tag,
                                                const double *__restrict__ bc, double omega,
@@ -672,9 +675,16 @@ __global__ void __launch_bounds__(BX, SHIFT ? LBGPU_PULL4H_SHIFT_MINB : 8) k_pul
     if (LBGPU_PF_ROWS > 0 && threadIdx.x == 0)
         prefetch_rows_l2<S, 4 * BX>(g, src, 1 + 4 * BX * (int)blockIdx.x, (int)blockIdx.y + 1 + LBGPU_PF_ROWS,
                                     LBGPU_PF_TAGS ? tag : nullptr);
+    if (PERIM_ROWS && (int)blockIdx.y >= g.ly) {   // the grid rows past the lattice: perimeter nodes
+        int X, Y;
+        const int p = (int)(((blockIdx.y - g.ly) * gridDim.x + blockIdx.x) * BX + threadIdx.x);
+        if (perim_node(g, p, X, Y))
+            pull_node<S, SHIFT ? 1 : 0, RS>(g, src, dst, tag, bc, omega, side, sc, inv, X, Y, g.rs_key);
+        return;
+    }
     const int t = blockIdx.x * BX + threadIdx.x;
-    pull_quad<S, SHIFT, RS, LBGPU_PULL4H_PERIM_APART != 0>(g, src, dst, tag, bc, omega, side, sc, inv, 1 + 4 * t,
-                                                          blockIdx.y + 1, threadIdx.x & 31, g.rs_key);
+    pull_quad<S, SHIFT, RS, PERIM_APART>(g, src, dst, tag, bc, omega, side, sc, inv, 1 + 4 * t, blockIdx.y + 1,
+                                         threadIdx.x & 31, g.rs_key);
 }
 
 // Propagation of C_n in `src` into `dst` (form C -> form L), ghost ring included; stale
@@ -1369,15 +1379,15 @@ __device__ __forceinline__ void batch_strip(const BatchInst *__restrict__ insts,
     }
     if constexpr (KIND == BATCH_PERIM) {
         if constexpr (sizeof(S) == 2) {
-            // the member's perimeter (perim_node numbering)
+            // a run of BT of the member's perimeter nodes (perim_node numbering)
             const int src = d.cur0 ^ (k & 1);
             const S *sb = static_cast<const S *>(d.buf[src]);
             S *db = static_cast<S *>(d.buf[src ^ 1]);
             const bool rs = RS && d.rs;
             const unsigned key = rs ? rs_key(d.rs_seed, (unsigned long long)(d.tau0 + k)) : 0u;
-            for (int p = threadIdx.x; p < 2 * g.lx + 2 * g.ly; p += BT) {
+            {   // perimeter nodes it.x0 .. it.x0 + BT - 1, one a thread
                 int X, Y;
-                if (!perim_node(g, p, X, Y)) continue;
+                if (!perim_node(g, it.x0 + (int)threadIdx.x, X, Y)) return;
                 if (RS && rs) {
                     if (SHQ && g.shift_u) pull_node<S, 1, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, X, Y, key);
                     else pull_node<S, 0, true>(g, sb, db, d.tag, d.bc, omega, side, sc, inv, X, Y, key);
@@ -1834,11 +1844,25 @@ void launch_collide_inplace(const DevLattice &d, int cur, int side_par, cudaStre
 template <class S, bool SHIFT, bool RS>
 static void launch_pull4h_t(const DevLattice &d, dim3 grid, int src, int side_par, cudaStream_t s)
 {
-    k_pull4h<S, SHIFT, RS><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
-                                               SIDE<S>(d, side_par), d.scale, d.inv_scale);
-    if (LBGPU_PULL4H_PERIM_APART)
+    if (!LBGPU_PULL4H_PERIM_APART) {
+        k_pull4h<S, SHIFT, RS><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
+                                                   SIDE<S>(d, side_par), d.scale, d.inv_scale);
+        return;
+    }
+    // the perimeter as extra grid rows of the same launch where CUDA's 65535 grid rows allow,
+    // else as a launch of its own after the quads
+    const int pblocks = cdiv(2 * d.g.lx + 2 * d.g.ly, BX);
+    const int prows = cdiv(pblocks, (int)grid.x);
+    if ((long long)grid.y + prows <= 65535) {
+        dim3 g2(grid.x, grid.y + prows);
+        k_pull4h<S, SHIFT, RS, true, true><<<g2, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc,
+                                                             d.omega, SIDE<S>(d, side_par), d.scale, d.inv_scale);
+    } else {
+        k_pull4h<S, SHIFT, RS, true, false><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc,
+                                                                d.omega, SIDE<S>(d, side_par), d.scale, d.inv_scale);
         k_perim_pull<S, SHIFT ? 1 : 0, RS><<<cdiv(2 * d.g.lx + 2 * d.g.ly, 256), 256, 0, s>>>(
             d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega, SIDE<S>(d, side_par), d.scale, d.inv_scale);
+    }
 }
 
 template <class S>
@@ -1856,7 +1880,10 @@ static void launch_pull4h(const DevLattice &d, dim3 grid, int src, int side_par,
 int pull_launches(const DevLattice &d, bool ghosts)
 {
     const bool half = d.precision == LBGPU_F16 || d.precision == LBGPU_BF16;
-    return (!ghosts && half && LBGPU_PULL4H_PERIM_APART) ? 2 : 1;
+    if (ghosts || !half || !LBGPU_PULL4H_PERIM_APART) return 1;
+    const int gx = cdiv((d.g.lx + 3) / 4, BX);
+    const int prows = cdiv(cdiv(2 * d.g.lx + 2 * d.g.ly, BX), gx);
+    return (long long)d.g.ly + prows <= 65535 ? 1 : 2;
 }
 
 void launch_pull(const DevLattice &d, int src, int side_par, bool ghosts, cudaStream_t s)

@@ -73,8 +73,8 @@ void launch_velocity_change(const DevLattice &d, int view, int cur, int side_par
 // threads per block = nodes per tile: 128, 256 or 512
 // Kinds of batch step: pull (one node per thread), AA even and odd, the 16-bit pull with four
 // nodes per thread (each warp one row of 128 nodes, see pull_quad), which leaves each member's
-// perimeter nodes to BATCH_PERIM: the pull step of those nodes, one per thread, one block a
-// member (work item: the member; its block loops over the perimeter).
+// perimeter nodes to BATCH_PERIM: the pull step of those nodes, one per thread, one block a run
+// of `threads` perimeter nodes of a member (work item: the member, x0 = the run's first number).
 enum { BATCH_PULL = 0, BATCH_AA_EVEN = 1, BATCH_AA_ODD = 2, BATCH_PULL4 = 3, BATCH_PERIM = 4 };
 constexpr int BATCH_KINDS = 5;
 
