@@ -657,9 +657,15 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
     }
 }
 
+// Perimeter nodes stepped apart from the quads (see k_pull4h): 1 for the row-shifted forms only,
+// 2 for every form, 0 for none.  Measured on one B200 at 16384 x 4096 (GLUPS, apart / in the
+// quad warps): banded shift + stochastic 155-158 / 148-151, banded shift 161 / 158; FP16 170 /
+// 174, FP16 stochastic 166 / 172, BF16 171 / 174.
 #ifndef LBGPU_PULL4H_PERIM_APART
-#define LBGPU_PULL4H_PERIM_APART 1  // perimeter nodes stepped apart from the quads (see k_pull4h)
+#define LBGPU_PULL4H_PERIM_APART 1
 #endif
+template <bool SHIFT>
+constexpr bool pull4h_perim_apart() { return LBGPU_PULL4H_PERIM_APART == 2 || (LBGPU_PULL4H_PERIM_APART == 1 && SHIFT); }
 #ifndef LBGPU_PULL4H_SHIFT_MINB
 #define LBGPU_PULL4H_SHIFT_MINB 7   // resident blocks of the row-shifted form (72 registers)
 #endif
@@ -1844,7 +1850,7 @@ void launch_collide_inplace(const DevLattice &d, int cur, int side_par, cudaStre
 template <class S, bool SHIFT, bool RS>
 static void launch_pull4h_t(const DevLattice &d, dim3 grid, int src, int side_par, cudaStream_t s)
 {
-    if (!LBGPU_PULL4H_PERIM_APART) {
+    if (!pull4h_perim_apart<SHIFT>()) {
         k_pull4h<S, SHIFT, RS><<<grid, BX, 0, s>>>(d.g, B<S>(d, src), B<S>(d, 1 - src), d.tag, d.bc, d.omega,
                                                    SIDE<S>(d, side_par), d.scale, d.inv_scale);
         return;
@@ -1880,7 +1886,8 @@ static void launch_pull4h(const DevLattice &d, dim3 grid, int src, int side_par,
 int pull_launches(const DevLattice &d, bool ghosts)
 {
     const bool half = d.precision == LBGPU_F16 || d.precision == LBGPU_BF16;
-    if (ghosts || !half || !LBGPU_PULL4H_PERIM_APART) return 1;
+    const bool apart = d.g.shift_u ? pull4h_perim_apart<true>() : pull4h_perim_apart<false>();
+    if (ghosts || !half || !apart) return 1;
     const int gx = cdiv((d.g.lx + 3) / 4, BX);
     const int prows = cdiv(cdiv(2 * d.g.lx + 2 * d.g.ly, BX), gx);
     return (long long)d.g.ly + prows <= 65535 ? 1 : 2;
