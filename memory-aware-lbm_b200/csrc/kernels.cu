@@ -666,8 +666,12 @@ __device__ __forceinline__ void pull_quad(const Geo &g, const S *__restrict__ sr
 #endif
 template <bool SHIFT>
 constexpr bool pull4h_perim_apart() { return LBGPU_PULL4H_PERIM_APART == 2 || (LBGPU_PULL4H_PERIM_APART == 1 && SHIFT); }
+// Resident blocks of the row-shifted form: 8 (64 registers) since its perimeter runs apart from
+// the quads (the quad path then spills 28-48 bytes); measured on one B200 at 16384 x 4096, banded
+// shift + stochastic 165.4-165.8 GLUPS against 162.3-162.4 at 7 blocks (72 registers), exact
+// profile + stochastic 151-153 against 143-144.
 #ifndef LBGPU_PULL4H_SHIFT_MINB
-#define LBGPU_PULL4H_SHIFT_MINB 7   // resident blocks of the row-shifted form (72 registers)
+#define LBGPU_PULL4H_SHIFT_MINB 8
 #endif
 // PERIM_APART: the quads leave the perimeter to another pass (see pull_quad); PERIM_ROWS: that pass
 // is the grid rows past the lattice's ly rows, one perimeter node a thread, so it runs inside the
