@@ -60,7 +60,7 @@ def parse():
                    help="pull2: the pull scheme with two steps per sweep (temporal blocking)")
     p.add_argument("--variants", default="auto",
                    help="comma list of precision:scheme also timed, 'auto' or 'none'")
-    p.add_argument("--study", choices=["batching", "serving", "precision"], default=None,
+    p.add_argument("--study", choices=["batching", "shapes", "serving", "precision"], default=None,
                    help="run a workload study instead of the headline benchmark (one GPU)")
     p.add_argument("--study-args", default="",
                    help="comma-separated key=value overrides of the study's defaults")
@@ -451,8 +451,8 @@ def run_study(args, dist):
                 kw[k] = float(v) if v.replace(".", "", 1).replace("e-", "", 1).isdigit() else v
     if dist.rank != 0:
         return
-    fn = {"batching": studies.batching_study, "serving": studies.serving_study,
-          "precision": studies.precision_study}[args.study]
+    fn = {"batching": studies.batching_study, "shapes": studies.member_shape_study,
+          "serving": studies.serving_study, "precision": studies.precision_study}[args.study]
     t0 = time.time()
     with ClockSampler(dist.local) as cs:
         res = fn(**kw)

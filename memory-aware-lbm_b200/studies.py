@@ -4,9 +4,14 @@ Every number comes from the library's kernels through lbgpu.py; the inputs are s
 cylinder channels (bounce-back walls, Poiseuille inlet, constant-density outlet).
 
 batching   independent channels of uneven size, Reynolds number and obstacle placement stepped
-           together (one persistent launch per step, CUDA-graph chunks of 50 steps, tile shapes
-           and pull/AA chosen per size class by the autotuners) against a sequential loop that
-           steps each channel alone with its own launches.
+           together (one launch per work list and step, persistent or one block per strip as
+           the autotuner picks, CUDA-graph chunks of 50 steps, tile shapes and pull/AA chosen per
+           size class by the autotuners) against a sequential loop that steps each channel
+           alone with its own launches.
+shapes     the batch's speed against its members' size and shape at a constant node count:
+           one large channel stepped alone, then batches of equal members, from one member of
+           the whole size down to many small ones, and members of equal area from wide and
+           short to narrow and tall.
 serving    a Poisson stream of channel requests through lbgpu_server: continuous batching under
            an HBM budget against sequential plain solves of the same requests; p50/p99 latency,
            aggregate MLUPS, and the velocity error of a sample against FP64 re-runs.
@@ -131,6 +136,68 @@ def batching_study(precisions=("f32", "f16"), n=512, steps=2000, seed=20260101, 
             "persistent": persistent, "threads_per_tile": threads,
             "autotune_best_ms": [round(x, 4) for x in best]}
     return res
+
+
+def member_shape_cases(total=16384 * 4096):
+    """(label, lx, ly, members) of the shapes study: members of total / 1, 16, 256, 1024 nodes
+    with lx = 4 ly, then 256 members of total / 256 nodes from 16:1 wide to 1:4 tall."""
+    cases = [("alone", 16384, 4096, 1)]
+    for lx, ly in ((16384, 4096), (4096, 1024), (1024, 256), (512, 128)):
+        cases.append(("size", lx, ly, max(1, total // (lx * ly))))
+    for lx, ly in ((4096, 64), (1024, 256), (512, 512), (256, 1024)):
+        cases.append(("shape", lx, ly, max(1, total // (lx * ly))))
+    return cases
+
+
+def shape_obstacle(lx, ly):
+    """Obstacle (x, y, r) of a shapes-study member: the benchmark's placement, with the radius
+    taken from the shorter side so that narrow members keep it clear of the inlet."""
+    return lx // 5 + 1, ly // 2 + 1, max(2, min(lx, ly) // 10 + 1)
+
+
+def member_shape_study(precision="f16", steps=100, passes=4, total=16384 * 4096):
+    """Device-timed MLUPS (best of three timings of `steps` steps after 50 warm-up steps) of each
+    case of member_shape_cases; 16-bit members run in quad tiles of 128 x 4, FP32/FP64 members
+    in the batch's default tiles; strips of `passes` tiles."""
+    def make(lx, ly):
+        lat = lbgpu.Lattice(lx, ly, precision, "pull")
+        if precision in lbgpu.DEFAULT_SCALE:
+            lat.set_offset_scale(lbgpu.DEFAULT_SCALE[precision])
+        ox, oy, r = shape_obstacle(lx, ly)
+        lat.setup_cylinder(ox, oy, r, 0.02, 100.0, lbgpu.WALL_BOUNCEBACK, lbgpu.OUTLET_CONST)
+        return lat
+
+    out = []
+    for label, lx, ly, n in member_shape_cases(total):
+        rec = {"case": label, "lx": lx, "ly": ly, "members": n,
+               "perimeter_share": round((2 * lx + 2 * ly - 4) / (lx * ly), 5)}
+        lats = []
+        try:
+            if label == "alone":
+                lats.append(make(lx, ly))
+                lats[0].step(20)
+                lats[0].synchronize()
+                ms = min(lats[0].step_timed(steps) for _ in range(3))
+            else:
+                lats = [make(lx, ly) for _ in range(n)]
+                with lbgpu.Batch(precision) as b:
+                    for c in range(6):
+                        if precision in ("f16", "bf16"):
+                            b.set_shape(c, 128, 4)
+                        b.set_passes(c, passes)
+                    for l in lats:
+                        b.add(l)
+                    b.step(50)
+                    b.synchronize()
+                    ms = min(b.step_timed(steps) for _ in range(3))
+        finally:
+            for l in lats:
+                l.close()
+        rec["mlups"] = round(n * lx * ly * steps / (ms * 1e-3) / 1e6, 1)
+        rec["gbs_algorithmic"] = round(rec["mlups"] * 1e6 * BYTES_PER_UPDATE[precision] / 1e9, 1)
+        out.append(rec)
+        _progress(f"shapes {label} {n} x {lx}x{ly}", rec)
+    return {"precision": precision, "steps": steps, "passes": passes, "nodes": total, "cases": out}
 
 
 # ------------------------------------------------------------------------------------------

@@ -30,3 +30,17 @@ def test_serving_umax_keeps_omega_at_or_below_the_edge():
             assert omega <= studies.OMEGA_MAX + 1e-12
         if q["umax"] > lo:   # raised only as far as needed
             assert omega >= studies.OMEGA_MAX - 1e-9 or q["umax"] == hi
+
+
+def test_member_shape_cases_hold_the_node_count_and_their_obstacles():
+    total = 16384 * 4096
+    cases = studies.member_shape_cases(total)
+    assert cases[0] == ("alone", 16384, 4096, 1)
+    for label, lx, ly, n in cases:
+        assert n * lx * ly == total, (label, lx, ly, n)
+        ox, oy, r = studies.shape_obstacle(lx, ly)
+        # the disk stays inside the interior, clear of the inlet column and the walls
+        assert 1 < ox - r and ox + r < lx and 1 < oy - r and oy + r < ly, (lx, ly, ox, oy, r)
+    shapes = [(lx, ly) for label, lx, ly, _ in cases if label == "shape"]
+    assert len({lx * ly for lx, ly in shapes}) == 1
+    assert shapes[0][0] > shapes[0][1] and shapes[-1][0] < shapes[-1][1]   # wide to tall
