@@ -1309,10 +1309,11 @@ __global__ void __launch_bounds__(BX, SHIFT ? LBGPU_AA4_ODD_MINB - 1 : LBGPU_AA4
 // the nine source and nine destination plane addresses live across iterations, which doubled the
 // registers per thread (and halved the resident warps) of the loop form.  Larger tiles instead
 // spread the two dependent descriptor loads at the start of a tile over more nodes.  The kernel
-// is bound by memory latency at the occupancy its registers allow (ncu: 62 % of warps active
-// at 40 registers against 86 % for the single-lattice pull kernel at 32), so the minimum blocks
-// per SM below cap the registers as far as that costs no (or a few bytes of) spills: 2048
-// threads a SM leave 32 registers a thread, 1280 leave 48, 1024 leave 64, 768 leave 80.
+// is bound by memory latency at the occupancy its registers allow (ncu, FP32 pull list: 62 % of
+// warps active at 40 registers before the cap, 84 % at 32 with it, against 86 % for the
+// single-lattice pull kernel), so the minimum blocks per SM below cap the registers as far as
+// that costs no (or a few bytes of) spills: 2048 threads a SM leave 32 registers a thread, 1280
+// leave 48, 1024 leave 64, 768 leave 80.
 // The 16-bit quad list: 8 blocks of 128 threads (64 registers, with spills) measured 96.8 GLUPS
 // on the 512-channel batch against 95.5 at 6 blocks (80 registers), 88.5 at 5 and 79.4 at 4
 // (127 registers, no spills): occupancy beats the spills here.
