@@ -2,13 +2,13 @@
 //
 // Requests (a cylinder channel, a step cap and a steady-state tolerance) arrive over wall-clock
 // time.  The loop admits them in arrival order while their lattices fit the HBM budget, keeps
-// every admitted lattice resident, advances them `check_every` steps at a time, and after each advance
-// retires every member that reached its step cap or whose largest velocity change over those
-// steps fell below its tolerance (device reduction, one copy back for all members).  Retiring
-// frees the member's memory, which admits waiting requests at the next round.  Lattices below
-// the solo size are members of one batch (one launch per step for all of them); larger ones,
-// which fill the GPU on their own, step with the single-lattice kernels on their own streams,
-// concurrently with the batch.
+// every admitted lattice resident, advances them `check_every` steps at a time, and after each
+// advance retires every member that reached its step cap or whose largest velocity change over
+// those steps fell below its tolerance (device reduction, one copy back for all members).
+// Retiring frees the member's memory, which admits waiting requests before the next advance.
+// Lattices below the solo size are members of one batch (one launch per step for all of them);
+// larger ones, which fill the GPU on their own, step with the single-lattice kernels on their
+// own streams, concurrently with the batch.
 //
 // The sequential mode serves the same requests one at a time, each stepped on its own
 // (plain solves: the single-lattice kernels, no batch, no graphs), as the comparison.
